@@ -1,0 +1,133 @@
+// c2q_host.h -- host-side objects behind the C ABI: context (stream, reduction
+// scratch, device scalars), gauge fields in every storage precision, eo spinor
+// fields, and the launch wrappers the solvers are built from.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cl2qcd_b200.h"
+#include "c2q_internal.cuh"
+#include "reduce.cuh"
+
+namespace c2q {
+
+struct Field;
+
+// Storage of one gauge field in one precision / compression.
+struct GaugeStore {
+    void* data = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace c2q
+
+struct c2q_ctx {
+    int device        = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream   = false;
+    std::string err;
+    long long launches = 0;
+    // reduction scratch (partials), the last-block ticket and result slots
+    double* partials       = nullptr;
+    size_t partials_cap    = 0;  // doubles
+    unsigned* ticket       = nullptr;
+    double* red_result     = nullptr;  // 8 doubles
+    double* host_pinned    = nullptr;  // 64 doubles, pinned
+    c2q::SolverScalars* scalars = nullptr;  // device solver scalars (one set per context)
+    // staging buffer for AoS host <-> device transfers
+    void* staging          = nullptr;
+    size_t staging_cap     = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct c2q_gauge {
+    c2q_ctx* ctx = nullptr;
+    c2q_lattice lat{};
+    c2q::Geom geom{};
+    // [0] FP64 18-real, [1] FP64 12-real, [2] FP32 18-real, [3] FP32 12-real, [4] FP16 12-real
+    c2q::GaugeStore store[5];
+};
+
+struct c2q_spinor_eo {
+    c2q_ctx* ctx = nullptr;
+    c2q_lattice lat{};
+    c2q::Geom geom{};
+    int prec   = 64;
+    void* data = nullptr;
+    float* norm = nullptr;  // FP16 only
+    bool owned = true;
+};
+
+namespace c2q {
+
+enum GaugeKind { G64 = 0, G64R12 = 1, G32 = 2, G32R12 = 3, G16R12 = 4 };
+
+// ---- status plumbing ----
+int fail(c2q_ctx* ctx, int code, const std::string& msg);
+int cuda_fail(c2q_ctx* ctx, cudaError_t e, const char* where);
+#define C2Q_CUDA(ctx, call)                                   \
+    do {                                                      \
+        cudaError_t _e = (call);                              \
+        if (_e != cudaSuccess) return ::c2q::cuda_fail((ctx), _e, #call); \
+    } while (0)
+
+// ---- geometry / coefficients ----
+bool make_geom(const c2q_lattice& lat, Geom* g);
+bool same_lattice(const c2q_lattice& a, const c2q_lattice& b);
+// Hop coefficients for one launch: -kappa * boundary phase (and chemical potential on T).
+HopCoef hop_coef(const c2q_lattice& lat, double kappa);
+EpiArgs diag_epi(double mubar, int which, int gamma5);
+
+// ---- fields ----
+// Allocate a spinor field of storage precision `prec` (stream-ordered allocation).
+int field_alloc(c2q_ctx* ctx, const c2q_lattice& lat, int prec, c2q_spinor_eo* f);
+void field_free(c2q_spinor_eo* f);
+size_t field_bytes(const Geom& g, int prec);
+int gauge_ensure(c2q_gauge* g, int kind);  // builds a lower-precision copy on first use
+int ensure_staging(c2q_ctx* ctx, size_t bytes);
+int ensure_partials(c2q_ctx* ctx, size_t blocks);
+
+template <int P>
+inline SpinorPtr<P> sptr(const c2q_spinor_eo* f)
+{
+    return SpinorPtr<P>{f ? f->data : nullptr, f ? f->norm : nullptr};
+}
+
+// ---- launches (all stream-ordered on ctx->stream) ----
+struct DotSpec {
+    int mode = 0;  // DotMode
+    const c2q_spinor_eo* y = nullptr;
+    int fin = FIN_STORE_RESULT;
+};
+
+// One dslash parity sweep at the fields' storage precision P.
+int launch_dslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_eo* out, const c2q_spinor_eo* in,
+                  int out_parity, double kappa, int epi, const EpiArgs& e, const c2q_spinor_eo* x,
+                  const DotSpec& dot);
+struct BlasSpec {
+    int op = 0;
+    Coef a{0, 0, nullptr, 1}, b{0, 0, nullptr, 1};
+    c2q_spinor_eo* out = nullptr;
+    const c2q_spinor_eo *x = nullptr, *y = nullptr, *z = nullptr;
+    int dot = 0;
+    int fin = FIN_STORE_RESULT;
+};
+int launch_blas(c2q_ctx* ctx, const BlasSpec& s);
+int launch_cg_update(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* r, const c2q_spinor_eo* p,
+                     const c2q_spinor_eo* v);
+int launch_cg_p(c2q_ctx* ctx, c2q_spinor_eo* p, const c2q_spinor_eo* r);
+int launch_convert(c2q_ctx* ctx, c2q_spinor_eo* out, const c2q_spinor_eo* in);
+
+// Fermion matrix application at the fields' precision.  tmp1/tmp2 are
+// scratch fields of the same precision.  `dot` applies to the last sweep.
+int apply_operator(c2q_ctx* ctx, int op, c2q_spinor_eo* out, const c2q_gauge* g, int gkind,
+                   const c2q_spinor_eo* in, double kappa, double mubar, int action, c2q_spinor_eo* tmp1,
+                   c2q_spinor_eo* tmp2, const DotSpec& dot, int* sweeps);
+
+// Read back `n` doubles of device memory synchronously through pinned memory.
+int read_scalars(c2q_ctx* ctx, const double* dev, int n, double* host);
+
+}  // namespace c2q

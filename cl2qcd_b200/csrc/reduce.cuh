@@ -1,0 +1,142 @@
+// reduce.cuh -- deterministic global reductions fused into the producing kernel.
+//
+// Every reducing kernel writes one partial per block into a scratch array, in
+// block order.  The last block to finish (an atomic ticket, reset by that
+// block) sums the partials in a fixed order with a fixed tree, so the result
+// is independent of block scheduling and bitwise reproducible for a given
+// launch shape.  No floating-point atomics are used anywhere.
+//
+// The same last block then runs a small scalar "finisher" on the device
+// (complex divisions for CG/BiCGStab coefficients), so solver iterations need
+// no host round trip.
+#pragma once
+
+#include "c2q_internal.cuh"
+
+namespace c2q {
+
+constexpr int RED_THREADS = 256;
+
+// Sum NV doubles across the block; result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void block_sum(double v[NV], double* smem /* NV * 32 */)
+{
+#pragma unroll
+    for (int k = 0; k < NV; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) smem[k * 32 + warp] = v[k];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = lane < nw ? smem[k * 32 + lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            v[k] = t;
+        }
+    }
+    __syncthreads();
+}
+
+// Device scalars of the Krylov solvers (complex, as the reference keeps them
+// in Scalar<hmc_complex>, physics/algorithms/solvers/cg.cpp:290-302).
+struct SolverScalars {
+    double omega[2];     // CG: (r,r) of the previous iteration | BiCGStab: omega
+    double rho[2];       // CG: (p,Ap)                           | BiCGStab: rho
+    double rho_next[2];  // CG: (r,r) new                        | BiCGStab: (rhat, r_new)
+    double alpha[2];
+    double beta[2];
+    double tmp1[2], tmp2[2];
+    double resid;        // last |r|^2 written by a reducing kernel
+    double aux[2];       // extra reduction slot (BiCGStab (t,t), true residual, ...)
+    int flag;            // nonzero: a division by zero / NaN was seen
+};
+
+// What the last block does with the reduced value(s).
+enum Finisher : int {
+    FIN_STORE_RESULT = 0,  // result[0..NV) = sum
+    FIN_CG_ALPHA     = 1,  // rho = sum; alpha = omega / rho
+    FIN_CG_BETA      = 2,  // rho_next = (sum,0); resid = sum; beta = rho_next/omega; omega = rho_next
+    FIN_CG_OMEGA     = 3,  // omega = (sum,0) ; resid = sum  (refresh iteration, (r,r))
+};
+
+struct RedArgs {
+    double* partials;      // >= gridDim.x * NV doubles of scratch
+    unsigned* ticket;      // zero-initialised counter, reset by the last block
+    double* result;        // FIN_STORE_RESULT destination (NV doubles)
+    SolverScalars* sc;     // solver scalars for the CG finishers
+    int fin;
+};
+
+__device__ __forceinline__ void cdiv_store(double* out, const double* n, const double* d, int* flag)
+{
+    const double norm = d[0] * d[0] + d[1] * d[1];
+    if (!(norm > 0.0)) *flag = 1;
+    out[0] = (n[0] * d[0] + n[1] * d[1]) / norm;
+    out[1] = (n[1] * d[0] - n[0] * d[1]) / norm;
+}
+
+// Called by every thread of every block after block_sum (value in thread 0).
+template <int NV>
+__device__ __forceinline__ void finish_reduction(const double v[NV], const RedArgs& ra, double* smem)
+{
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) ra.partials[(size_t)blockIdx.x * NV + k] = v[k];
+        __threadfence();
+        const unsigned t = atomicAdd(ra.ticket, 1u);
+        last             = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // fixed-order sum of the partials: thread j takes a contiguous chunk
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    const int n = gridDim.x, chunk = (n + blockDim.x - 1) / blockDim.x;
+    const int lo = threadIdx.x * chunk, hi = min(n, lo + chunk);
+    for (int b = lo; b < hi; ++b)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(ra.partials + (size_t)b * NV + k);
+    block_sum<NV>(acc, smem);
+    if (threadIdx.x == 0) {
+        *ra.ticket = 0u;
+        SolverScalars* s = ra.sc;
+        switch (ra.fin) {
+            case FIN_STORE_RESULT:
+#pragma unroll
+                for (int k = 0; k < NV; ++k) ra.result[k] = acc[k];
+                break;
+            case FIN_CG_ALPHA: {
+                s->rho[0] = acc[0];
+                s->rho[1] = NV > 1 ? acc[NV > 1 ? 1 : 0] : 0.0;
+                cdiv_store(s->alpha, s->omega, s->rho, &s->flag);
+                break;
+            }
+            case FIN_CG_BETA: {
+                s->rho_next[0] = acc[0];
+                s->rho_next[1] = 0.0;
+                s->resid       = acc[0];
+                cdiv_store(s->beta, s->rho_next, s->omega, &s->flag);
+                s->omega[0] = s->rho_next[0];
+                s->omega[1] = s->rho_next[1];
+                break;
+            }
+            case FIN_CG_OMEGA: {
+                s->omega[0] = acc[0];
+                s->omega[1] = 0.0;
+                s->resid    = acc[0];
+                break;
+            }
+        }
+        __threadfence();
+    }
+}
+
+}  // namespace c2q

@@ -1,0 +1,715 @@
+// solvers.cu -- CG (FP64 and mixed precision with FP64 reliable updates),
+// BiCGStab (fast and save variants) and the eo Schur-complement inversion,
+// on top of the fused sweeps of fields.cu.
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#include "blas.cuh"
+#include "c2q_host.h"
+#include "mixed.cuh"
+
+namespace c2q {
+
+namespace {
+
+struct Cx {
+    double re, im;
+};
+inline Cx cdiv(Cx n, Cx d)
+{
+    // complexdivide, common_header_files/operations_complex.hpp:59-66
+    const double norm = d.re * d.re + d.im * d.im;
+    return {(n.re * d.re + n.im * d.im) / norm, (n.im * d.re - n.re * d.im) / norm};
+}
+inline Cx cmulx(Cx a, Cx b) { return {a.re * b.re - a.im * b.im, a.im * b.re + a.re * b.im}; }
+
+// RAII group of scratch fields
+struct Fields {
+    std::vector<c2q_spinor_eo> f;
+    ~Fields()
+    {
+        for (auto& x : f) field_free(&x);
+    }
+};
+
+int make_fields(c2q_ctx* ctx, const c2q_lattice& lat, int prec, int n, Fields& F, size_t first)
+{
+    F.f.resize(first + n);
+    for (int k = 0; k < n; ++k) {
+        int rc = field_alloc(ctx, lat, prec, &F.f[first + k]);
+        if (rc) return rc;
+    }
+    return C2Q_OK;
+}
+
+struct SolveClock {
+    c2q_ctx* ctx;
+    explicit SolveClock(c2q_ctx* c) : ctx(c) { cudaEventRecord(ctx->ev0, ctx->stream); }
+    double seconds()
+    {
+        cudaEventRecord(ctx->ev1, ctx->stream);
+        cudaEventSynchronize(ctx->ev1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        return ms * 1e-3;
+    }
+};
+
+int read_sc(c2q_ctx* ctx, SolverScalars* h)
+{
+    C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, ctx->scalars, sizeof(SolverScalars), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    memcpy(h, ctx->host_pinned, sizeof(SolverScalars));
+    return C2Q_OK;
+}
+
+int write_sc(c2q_ctx* ctx, const SolverScalars& h)
+{
+    memcpy(ctx->host_pinned, &h, sizeof(SolverScalars));
+    C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->scalars, ctx->host_pinned, sizeof(SolverScalars), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return C2Q_OK;
+}
+
+// out = y - a x with |out|^2 into the reduction result (or a finisher); returns via read if asked
+int saxpy_norm(c2q_ctx* ctx, c2q_spinor_eo* out, Cx a, const c2q_spinor_eo* x, const c2q_spinor_eo* y, int fin,
+               double* norm_out)
+{
+    BlasSpec s;
+    s.op  = B_SAXPY;
+    s.out = out;
+    s.x   = x;
+    s.y   = y;
+    s.a   = coef_host(a.re, a.im);
+    s.dot = 2;
+    s.fin = fin;
+    int rc = launch_blas(ctx, s);
+    if (rc || !norm_out) return rc;
+    double h[2];
+    rc        = read_scalars(ctx, ctx->red_result, 2, h);
+    *norm_out = h[0];
+    return rc;
+}
+
+int dot_read(c2q_ctx* ctx, const c2q_spinor_eo* x, const c2q_spinor_eo* y, Cx* out)
+{
+    BlasSpec s;
+    s.x   = x;
+    s.y   = y;
+    s.dot = 1;
+    int rc = launch_blas(ctx, s);
+    if (rc) return rc;
+    double h[2];
+    rc   = read_scalars(ctx, ctx->red_result, 2, h);
+    *out = {h[0], h[1]};
+    return rc;
+}
+
+int copy_field(c2q_ctx* ctx, c2q_spinor_eo* to, const c2q_spinor_eo* from)
+{
+    BlasSpec s;
+    s.op  = B_COPY;
+    s.out = to;
+    s.x   = from;
+    return launch_blas(ctx, s);
+}
+
+int gkind_for(int prec, int rec12)
+{
+    if (prec == 64) return rec12 ? G64R12 : G64;
+    if (prec == 32) return rec12 ? G32R12 : G32;
+    return G16R12;
+}
+
+// ||b - A x||^2 in FP64 (true residual); r receives b - A x.
+int true_residual(c2q_ctx* ctx, int op, const c2q_gauge* g, const c2q_spinor_eo* x, const c2q_spinor_eo* b,
+                  double kappa, double mubar, int action, c2q_spinor_eo* r, c2q_spinor_eo* t1, c2q_spinor_eo* t2,
+                  double* r2, int* sweeps)
+{
+    int rc = apply_operator(ctx, op, r, g, G64, x, kappa, mubar, action, t1, t2, DotSpec{}, sweeps);
+    if (rc) return rc;
+    return saxpy_norm(ctx, r, Cx{1, 0}, r, b, FIN_STORE_RESULT, r2);
+}
+
+bool validate(c2q_ctx* ctx, const c2q_spinor_eo* x, const c2q_gauge* g, const c2q_spinor_eo* b,
+              const c2q_solver_params* p, int* rc)
+{
+    if (!x || !g || !b || !p) {
+        *rc = C2Q_BAD_ARG;
+        return false;
+    }
+    if (x->prec != 64 || b->prec != 64 || !same_lattice(x->lat, b->lat) || !same_lattice(x->lat, g->lat)) {
+        *rc = fail(ctx, C2Q_BAD_ARG, "solver fields must be FP64 fields on the gauge field's lattice");
+        return false;
+    }
+    if (p->iter_refresh <= 0 || p->resid_check_every <= 0 || p->cgmax < 0) {
+        *rc = fail(ctx, C2Q_BAD_ARG, "solverRestartEvery and solverResiduumCheckEvery must be positive");
+        return false;
+    }
+    if (p->precision != 64 && p->precision != 32 && p->precision != 16) {
+        *rc = fail(ctx, C2Q_BAD_ARG, "precision must be 64, 32 or 16");
+        return false;
+    }
+    return true;
+}
+
+double stop_threshold(const c2q_solver_params* p, double b2)
+{
+    double thr = 0.0;
+    if (p->prec > 0) thr = p->prec;
+    if (p->rel_tol > 0) thr = std::max(thr, p->rel_tol * p->rel_tol * b2);
+    return thr;
+}
+
+void finish_report(c2q_solve_report* rep, int status, int iters, int rel, double r2, double true_rel, double secs,
+                   int sweeps)
+{
+    if (!rep) return;
+    rep->status              = status;
+    rep->iterations          = iters;
+    rep->reliable_updates    = rel;
+    rep->resid_sq            = r2;
+    rep->true_resid_rel      = true_rel;
+    rep->seconds             = secs;
+    rep->dslash_applications = sweeps;
+}
+
+// ------------------------------------------------------------------ FP64 CG
+// physics/algorithms/solvers/cg.cpp:277-400 with device-resident scalars.
+int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
+            double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
+{
+    Fields F;
+    int rc = make_fields(ctx, x->lat, 64, 5, F, 0);
+    if (rc) return rc;
+    c2q_spinor_eo *p = &F.f[0], *rn = &F.f[1], *v = &F.f[2], *t1 = &F.f[3], *t2 = &F.f[4];
+    const int gk = gkind_for(64, P->use_rec12);
+    int sweeps   = 0;
+    SolveClock clock(ctx);
+
+    double b2 = 0;
+    rc        = saxpy_norm(ctx, rn, Cx{0, 0}, b, b, FIN_STORE_RESULT, &b2);
+    if (rc) return rc;
+    const double thr = stop_threshold(P, b2);
+    SolverScalars zero{};
+    rc = write_sc(ctx, zero);
+    if (rc) return rc;
+
+    int iter = 0, status = C2Q_DID_NOT_SOLVE;
+    double resid = std::numeric_limits<double>::quiet_NaN();
+    bool force_refresh = false;
+    for (iter = 0; iter < P->cgmax || iter < P->min_iter; iter++) {
+        if (iter % P->iter_refresh == 0 || force_refresh) {
+            force_refresh = false;
+            rc = apply_operator(ctx, op, rn, g, gk, x, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
+            if (!rc) rc = saxpy_norm(ctx, rn, Cx{1, 0}, rn, b, FIN_CG_OMEGA, nullptr);  // rn = b - A x ; omega = (rn,rn)
+            if (!rc) rc = copy_field(ctx, p, rn);
+            if (rc) return rc;
+        }
+        DotSpec d;
+        d.mode = DOT_Y;
+        d.y    = p;
+        d.fin  = FIN_CG_ALPHA;  // rho = (p, v) ; alpha = omega / rho
+        rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
+        if (!rc) rc = launch_cg_update(ctx, x, rn, p, v);  // x += alpha p ; rn -= alpha v ; beta, omega
+        if (rc) return rc;
+        if (iter % P->resid_check_every == 0) {
+            SolverScalars h;
+            rc = read_sc(ctx, &h);
+            if (rc) return rc;
+            resid = h.resid;
+            if (resid != resid) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            if (resid < thr && iter >= P->min_iter) {
+                if (P->rel_tol > 0) {
+                    double r2t = 0;
+                    rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, t2, t1, v, &r2t, &sweeps);
+                    if (rc) return rc;
+                    if (r2t <= P->rel_tol * P->rel_tol * b2 || (P->prec > 0 && r2t < P->prec)) {
+                        status = iter;
+                        break;
+                    }
+                    force_refresh = true;  // iterated residual drifted: restart from the true residual
+                    continue;
+                }
+                status = iter;
+                break;
+            }
+        }
+        rc = launch_cg_p(ctx, p, rn);  // p = rn + beta p
+        if (rc) return rc;
+    }
+    double r2t = 0;
+    rc         = true_residual(ctx, op, g, x, b, kappa, mubar, action, rn, t1, t2, &r2t, &sweeps);
+    if (rc) return rc;
+    finish_report(rep, status, iter, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sweeps);
+    if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
+    if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "NAN occured in the CG residual");
+    return status;
+}
+
+// ------------------------------------------------------- mixed-precision CG
+// CG in reduced precision PB (operator, search direction) / FP32 (residual,
+// solution increment), with FP64 reliable updates: whenever the iterated
+// residual has dropped by `reliable_delta` since the last update (or reached
+// the stopping threshold), the increment is added to the FP64 solution and the
+// residual is recomputed from scratch in FP64 with FP64 links.
+template <int PB>
+int mix_update(c2q_ctx* ctx, c2q_spinor_eo* xs, c2q_spinor_eo* rs, const c2q_spinor_eo* p, const c2q_spinor_eo* v)
+{
+    MixUpdateArgs<32, PB> A;
+    A.x      = sptr<32>(xs);
+    A.r      = sptr<32>(rs);
+    A.p      = sptr<PB>(p);
+    A.v      = sptr<PB>(v);
+    A.sc     = ctx->scalars;
+    A.n      = xs->geom.seo;
+    A.stride = xs->geom.stride;
+    const int blocks = (A.n + BLAS_THREADS - 1) / BLAS_THREADS;
+    int rc           = ensure_partials(ctx, blocks);
+    if (rc) return rc;
+    A.red.partials = ctx->partials;
+    A.red.ticket   = ctx->ticket;
+    A.red.result   = ctx->red_result;
+    A.red.sc       = ctx->scalars;
+    A.red.fin      = FIN_CG_BETA;
+    mix_update_kernel<32, PB><<<blocks, BLAS_THREADS, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    C2Q_CUDA(ctx, cudaGetLastError());
+    return C2Q_OK;
+}
+
+template <int PB>
+int mix_p(c2q_ctx* ctx, c2q_spinor_eo* p, const c2q_spinor_eo* rs)
+{
+    MixPArgs<32, PB> A;
+    A.p      = sptr<PB>(p);
+    A.r      = sptr<32>(rs);
+    A.sc     = ctx->scalars;
+    A.n      = p->geom.seo;
+    A.stride = p->geom.stride;
+    mix_p_kernel<32, PB><<<(A.n + BLAS_THREADS - 1) / BLAS_THREADS, BLAS_THREADS, 0, ctx->stream>>>(A);
+    ctx->launches++;
+    C2Q_CUDA(ctx, cudaGetLastError());
+    return C2Q_OK;
+}
+
+int accumulate(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* xs)
+{
+    const int n = x->geom.seo;
+    accumulate_kernel<32><<<(n + BLAS_THREADS - 1) / BLAS_THREADS, BLAS_THREADS, 0, ctx->stream>>>(
+        sptr<64>(x), sptr<32>(xs), n, x->geom.stride);
+    ctx->launches++;
+    C2Q_CUDA(ctx, cudaGetLastError());
+    return C2Q_OK;
+}
+
+template <int PB>
+int cg_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
+             double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
+{
+    Fields F;
+    int rc = make_fields(ctx, x->lat, 64, 3, F, 0);  // r64, t1_64, t2_64
+    if (!rc) rc = make_fields(ctx, x->lat, 32, 2, F, 3);  // rs, xs
+    if (!rc) rc = make_fields(ctx, x->lat, PB, 4, F, 5);  // p, v, t1, t2
+    if (rc) return rc;
+    c2q_spinor_eo *r64 = &F.f[0], *a64 = &F.f[1], *b64 = &F.f[2];
+    c2q_spinor_eo *rs = &F.f[3], *xs = &F.f[4];
+    c2q_spinor_eo *p = &F.f[5], *v = &F.f[6], *t1 = &F.f[7], *t2 = &F.f[8];
+    const int gk   = gkind_for(PB, P->use_rec12 || PB == 16);
+    rc             = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
+    if (rc) return rc;
+    const double delta = P->reliable_delta > 0 ? P->reliable_delta : 0.1;
+    int sweeps         = 0, reliable = 0;
+    SolveClock clock(ctx);
+
+    double b2 = 0;
+    rc        = saxpy_norm(ctx, r64, Cx{0, 0}, b, b, FIN_STORE_RESULT, &b2);
+    if (rc) return rc;
+    const double thr = stop_threshold(P, b2);
+    double r2        = 0;
+    rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
+    if (rc) return rc;
+    int iter = 0, status = C2Q_DID_NOT_SOLVE;
+    double resid = r2;
+    if (r2 < thr) {
+        status = 0;
+    } else {
+        rc = launch_convert(ctx, rs, r64);
+        if (!rc) rc = c2q_spinor_eo_zero(xs);
+        if (!rc) rc = launch_convert(ctx, p, rs);
+        SolverScalars s0{};
+        s0.omega[0] = r2;
+        if (!rc) rc = write_sc(ctx, s0);
+        if (rc) return rc;
+        double maxrr = std::sqrt(r2);
+        for (iter = 0; iter < P->cgmax; ++iter) {
+            DotSpec d;
+            d.mode = DOT_Y;
+            d.y    = p;
+            d.fin  = FIN_CG_ALPHA;
+            rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
+            if (!rc) rc = mix_update<PB>(ctx, xs, rs, p, v);
+            if (rc) return rc;
+            if (iter % P->resid_check_every == 0) {
+                SolverScalars h;
+                rc = read_sc(ctx, &h);
+                if (rc) return rc;
+                resid = h.resid;
+                if (resid != resid || h.flag) {
+                    status = C2Q_SOLVER_STUCK;
+                    break;
+                }
+                const double rn = std::sqrt(resid);
+                if (rn > maxrr) maxrr = rn;
+                if (rn < delta * maxrr || resid < thr) {
+                    // reliable update in FP64
+                    rc = accumulate(ctx, x, xs);
+                    if (!rc) rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
+                    if (rc) return rc;
+                    ++reliable;
+                    resid = r2;
+                    if (r2 < thr) {
+                        status = iter + 1;
+                        break;
+                    }
+                    rc = launch_convert(ctx, rs, r64);
+                    if (rc) return rc;
+                    maxrr = std::sqrt(r2);
+                    // keep the search direction; rescale beta to the true residual
+                    h.beta[0] *= r2 / h.resid;
+                    h.beta[1] *= r2 / h.resid;
+                    h.omega[0] = r2;
+                    h.omega[1] = 0.0;
+                    h.resid    = r2;
+                    rc         = write_sc(ctx, h);
+                    if (rc) return rc;
+                }
+            }
+            rc = mix_p<PB>(ctx, p, rs);
+            if (rc) return rc;
+        }
+        if (status == C2Q_DID_NOT_SOLVE || status == C2Q_SOLVER_STUCK) {
+            // keep what was gained
+            int rc2 = accumulate(ctx, x, xs);
+            if (rc2) return rc2;
+        }
+    }
+    double r2t = 0;
+    rc         = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2t, &sweeps);
+    if (rc) return rc;
+    finish_report(rep, status, iter, reliable, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sweeps);
+    if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
+    if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "NAN occured in the mixed-precision CG residual");
+    return status;
+}
+
+// ------------------------------------------------------------- BiCGStab
+// physics/algorithms/solvers/bicgstab.cpp:566-733 (fast) and :401-564 (save);
+// scalars are read back every iteration as the reference does.
+int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b,
+                  double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
+{
+    Fields F;
+    int rc = make_fields(ctx, x->lat, 64, 9, F, 0);
+    if (rc) return rc;
+    c2q_spinor_eo *p = &F.f[0], *rn = &F.f[1], *rhat = &F.f[2], *s = &F.f[3], *t = &F.f[4], *v = &F.f[5],
+                  *aux = &F.f[6], *t1 = &F.f[7], *t2 = &F.f[8];
+    const int gk  = gkind_for(64, P->use_rec12);
+    const bool save = P->solver == C2Q_SOLVER_BICGSTAB_SAVE;
+    int sweeps    = 0;
+    SolveClock clock(ctx);
+    double b2 = 0;
+    rc        = saxpy_norm(ctx, aux, Cx{0, 0}, b, b, FIN_STORE_RESULT, &b2);
+    if (rc) return rc;
+    const double thr = stop_threshold(P, b2);
+    const Cx one{1, 0}, mone{-1, 0};
+    Cx alpha{1, 0}, omega{1, 0}, rho{1, 0}, rho_next, beta, tmp1, tmp2;
+    double resid = std::numeric_limits<double>::quiet_NaN();
+    int iter = 0, status = C2Q_DID_NOT_SOLVE;
+
+    auto apply = [&](c2q_spinor_eo* out, const c2q_spinor_eo* in) {
+        return apply_operator(ctx, op, out, g, gk, in, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
+    };
+    auto saxsbypz = [&](c2q_spinor_eo* out, Cx a, const c2q_spinor_eo* xx, Cx bb, const c2q_spinor_eo* yy,
+                        const c2q_spinor_eo* zz) {
+        BlasSpec sp;
+        sp.op  = B_SAXSBYPZ;
+        sp.out = out;
+        sp.x   = xx;
+        sp.y   = yy;
+        sp.z   = zz;
+        sp.a   = coef_host(a.re, a.im);
+        sp.b   = coef_host(bb.re, bb.im);
+        return launch_blas(ctx, sp);
+    };
+    auto saxpy = [&](c2q_spinor_eo* out, Cx a, const c2q_spinor_eo* xx, const c2q_spinor_eo* yy) {
+        BlasSpec sp;
+        sp.op  = B_SAXPY;
+        sp.out = out;
+        sp.x   = xx;
+        sp.y   = yy;
+        sp.a   = coef_host(a.re, a.im);
+        return launch_blas(ctx, sp);
+    };
+    auto sqnorm = [&](const c2q_spinor_eo* f, double* out) {
+        Cx c;
+        int r = dot_read(ctx, f, f, &c);
+        *out  = c.re;
+        return r;
+    };
+    // true-residual confirmation (used by the save variant and by rel_tol)
+    auto confirmed = [&](bool* ok) {
+        double tr = 0;
+        int r     = apply(aux, x);
+        if (!r) r = saxpy_norm(ctx, aux, one, aux, b, FIN_STORE_RESULT, &tr);
+        const double lim = P->rel_tol > 0 ? std::max(thr, 0.0) : P->prec;
+        *ok              = tr < (P->rel_tol > 0 ? std::max(P->rel_tol * P->rel_tol * b2, P->prec > 0 ? P->prec : 0.0)
+                                                 : lim);
+        return r;
+    };
+
+    if (!save) {
+        for (iter = 0; iter < P->cgmax; iter++) {
+            if (iter % P->iter_refresh == 0) {
+                rc = apply(rn, x);
+                if (!rc) rc = saxpy(p, one, rn, b);
+                if (!rc) rc = copy_field(ctx, rhat, p);
+                if (!rc) rc = copy_field(ctx, rn, p);
+                if (!rc) rc = dot_read(ctx, rhat, rn, &rho);
+                if (rc) return rc;
+            }
+            rc = sqnorm(rn, &resid);
+            if (rc) return rc;
+            if (resid != resid) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            if (resid < thr) {
+                bool ok = true;
+                if (P->rel_tol > 0) {
+                    rc = confirmed(&ok);
+                    if (rc) return rc;
+                }
+                if (ok) {
+                    status = iter;
+                    break;
+                }
+            }
+            rc = apply(v, p);
+            if (!rc) rc = dot_read(ctx, rhat, v, &tmp1);
+            if (rc) return rc;
+            alpha = cdiv(rho, tmp1);
+            rc    = saxpy(s, alpha, v, rn);
+            if (!rc) rc = apply(t, s);
+            if (!rc) rc = dot_read(ctx, t, s, &tmp1);
+            if (!rc) rc = dot_read(ctx, t, t, &tmp2);
+            if (rc) return rc;
+            omega = cdiv(tmp1, tmp2);
+            rc    = saxsbypz(x, alpha, p, omega, s, x);
+            if (!rc) rc = saxpy(rn, omega, t, s);
+            if (!rc) rc = dot_read(ctx, rhat, rn, &rho_next);
+            if (rc) return rc;
+            if (std::fabs(rho_next.re) < 1e-25 && std::fabs(rho_next.im) < 1e-25) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            tmp1 = cdiv(rho_next, rho);
+            tmp2 = cdiv(alpha, omega);
+            beta = cmulx(tmp1, tmp2);
+            tmp1 = cmulx(beta, omega);
+            tmp2 = cmulx(mone, tmp1);
+            rc   = saxsbypz(p, beta, p, tmp2, v, rn);
+            if (rc) return rc;
+            rho = rho_next;
+        }
+    } else {
+        for (iter = 0; iter < P->cgmax; iter++) {
+            if (iter % P->iter_refresh == 0) {
+                rc = c2q_spinor_eo_zero(v);
+                if (!rc) rc = c2q_spinor_eo_zero(p);
+                if (!rc) rc = apply(rn, x);
+                if (!rc) rc = saxpy(rn, one, rn, b);
+                if (!rc) rc = copy_field(ctx, rhat, rn);
+                if (rc) return rc;
+                alpha = one;
+                omega = one;
+                rho   = one;
+            }
+            rc = dot_read(ctx, rhat, rn, &rho_next);
+            if (rc) return rc;
+            if (std::fabs(rho_next.re) < 1e-25 && std::fabs(rho_next.im) < 1e-25) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            tmp1 = cdiv(rho_next, rho);
+            rho  = rho_next;
+            tmp2 = cdiv(alpha, omega);
+            beta = cmulx(tmp1, tmp2);
+            tmp1 = cmulx(beta, omega);
+            tmp2 = cmulx(mone, tmp1);
+            rc   = saxsbypz(p, beta, p, tmp2, v, rn);
+            if (!rc) rc = apply(v, p);
+            if (!rc) rc = dot_read(ctx, rhat, v, &tmp1);
+            if (rc) return rc;
+            alpha = cdiv(rho, tmp1);
+            rc    = saxpy(s, alpha, v, rn);
+            if (!rc) rc = apply(t, s);
+            if (!rc) rc = dot_read(ctx, t, s, &tmp1);
+            if (!rc) rc = dot_read(ctx, t, t, &tmp2);
+            if (rc) return rc;
+            omega = cdiv(tmp1, tmp2);
+            rc    = saxpy(rn, omega, t, s);
+            if (!rc) rc = saxsbypz(x, alpha, p, omega, s, x);
+            if (!rc) rc = sqnorm(rn, &resid);
+            if (rc) return rc;
+            if (resid != resid) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            if (resid < thr) {
+                bool ok = false;
+                rc      = confirmed(&ok);
+                if (rc) return rc;
+                if (ok) {
+                    status = iter;
+                    break;
+                }
+            }
+        }
+    }
+    double r2t = 0;
+    rc         = true_residual(ctx, op, g, x, b, kappa, mubar, action, aux, t1, t2, &r2t, &sweeps);
+    if (rc) return rc;
+    finish_report(rep, status, iter, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sweeps);
+    if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
+    if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "BiCGStab stuck (NaN residual or vanishing rho)");
+    return status;
+}
+
+}  // namespace
+}  // namespace c2q
+
+using namespace c2q;
+
+extern "C" {
+
+C2Q_EXPORT void c2q_solver_params_default(c2q_solver_params* p)
+{
+    if (!p) return;
+    p->solver            = C2Q_SOLVER_BICGSTAB;  // meta/parametersSolver.cpp:93
+    p->prec              = 1e-23;                // :76-78 (double precision build)
+    p->rel_tol           = 0.0;
+    p->cgmax             = 1000;                 // :85
+    p->iter_refresh      = 100;                  // :84
+    p->resid_check_every = 10;                   // :87
+    p->min_iter          = 0;
+    p->precision         = C2Q_PREC_FP64;
+    p->reliable_delta    = 0.1;
+    p->use_rec12         = 0;
+    p->use_graph         = 0;
+}
+
+C2Q_EXPORT int c2q_cg(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
+                      double mubar, int action, const c2q_solver_params* p, c2q_solve_report* report)
+{
+    if (!x) return C2Q_BAD_ARG;
+    c2q_ctx* ctx = x->ctx;
+    int rc       = 0;
+    if (!validate(ctx, x, g, b, p, &rc)) return rc;
+    if (x == b) return fail(ctx, C2Q_BAD_ARG, "solution and source must be different fields");
+    switch (p->precision) {
+        case 64: return cg_fp64(ctx, x, op, g, b, kappa, mubar, action, p, report);
+        case 32: return cg_mixed<32>(ctx, x, op, g, b, kappa, mubar, action, p, report);
+        default: return cg_mixed<16>(ctx, x, op, g, b, kappa, mubar, action, p, report);
+    }
+}
+
+C2Q_EXPORT int c2q_bicgstab(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
+                            double mubar, int action, const c2q_solver_params* p, c2q_solve_report* report)
+{
+    if (!x) return C2Q_BAD_ARG;
+    c2q_ctx* ctx = x->ctx;
+    int rc       = 0;
+    if (!validate(ctx, x, g, b, p, &rc)) return rc;
+    if (x == b) return fail(ctx, C2Q_BAD_ARG, "solution and source must be different fields");
+    return bicgstab_impl(ctx, x, op, g, b, kappa, mubar, action, p, report);
+}
+
+C2Q_EXPORT int c2q_cg_multi(c2q_spinor_eo* const* x, int op, const c2q_gauge* g, const c2q_spinor_eo* const* b,
+                            int nrhs, double kappa, double mubar, int action, const c2q_solver_params* p,
+                            c2q_solve_report* reports)
+{
+    if (!x || !b || nrhs <= 0) return C2Q_BAD_ARG;
+    int worst = 0;
+    for (int k = 0; k < nrhs; ++k) {
+        int rc = c2q_cg(x[k], op, g, b[k], kappa, mubar, action, p, reports ? &reports[k] : nullptr);
+        if (rc < 0 && (worst >= 0 || rc < worst)) worst = rc;
+    }
+    return worst < 0 ? worst : C2Q_OK;
+}
+
+// Eo branch of invert_M_nf2_upperflavour (physics/algorithms/inversion.cpp:129-236).
+C2Q_EXPORT int c2q_perform_inversion_eo(c2q_ctx* ctx, double* result, const c2q_gauge* g, const double* source,
+                                        double kappa, double mubar, int action, const c2q_solver_params* p,
+                                        c2q_solve_report* report)
+{
+    if (!ctx || !result || !g || !source || !p) return C2Q_BAD_ARG;
+    Fields F;
+    int rc = make_fields(ctx, g->lat, 64, 5, F, 0);
+    if (rc) return rc;
+    c2q_spinor_eo *src_even = &F.f[0], *src_odd = &F.f[1], *tmp1 = &F.f[2], *tmp2 = &F.f[3], *res = &F.f[4];
+    const bool tm = action == C2Q_ACTION_TWISTEDMASS;
+    // parity-role swap of the reference (issue #387 workaround, inversion.cpp:141-149)
+    rc = c2q_convert_to_eoprec(src_odd, src_even, source);
+    if (rc) return rc;
+    // b_e' = D M^{-1} b_o - b_e  (saxpy(&source_even, one, source_even, tmp), inversion.cpp:159-170)
+    if (tm) {
+        rc = c2q_tm_sitediagonal(tmp1, src_odd, mubar, C2Q_DIAG_M_TM_INVERSE);
+        if (!rc) rc = c2q_dslash_eo(tmp2, g, tmp1, C2Q_EVEN, kappa);
+        if (!rc) rc = c2q_saxpy(src_even, 1, 0, src_even, tmp2);
+    } else {
+        rc = c2q_dslash_eo(tmp1, g, src_odd, C2Q_EVEN, kappa);
+        if (!rc) rc = c2q_saxpy(src_even, 1, 0, src_even, tmp1);
+    }
+    if (!rc) rc = c2q_spinor_eo_cold(res);
+    if (rc) return rc;
+    c2q_solver_params pb = *p;
+    if (p->solver == C2Q_SOLVER_CG) pb.solver = C2Q_SOLVER_BICGSTAB;  // solver=cg tries BiCGStab first (:176-181)
+    int conv = c2q_bicgstab(res, C2Q_OP_AEE, g, src_even, kappa, mubar, action, &pb, report);
+    if (conv < 0 && conv != C2Q_SOLVER_STUCK && conv != C2Q_DID_NOT_SOLVE) return conv;
+    if (conv < 0) {
+        if (p->solver != C2Q_SOLVER_CG) return conv;
+        // CG fallback on QplusQminus_eo with g5 b, then x = Qminus_eo y (:182-195)
+        rc = c2q_gamma5_eo(src_even);
+        if (rc) return rc;
+        conv = c2q_cg(res, C2Q_OP_QPLUSQMINUS_EO, g, src_even, kappa, mubar, action, p, report);
+        if (conv < 0) return conv;
+        rc = c2q_apply_eo(C2Q_OP_QMINUS_EO, src_even, g, res, kappa, mubar, action, 0);
+        if (!rc) rc = c2q_copyData(res, src_even);
+        if (rc) return rc;
+    }
+    // x_o = -(M^{-1} D x_e + M^{-1} b_o)  (:204-221)
+    if (tm) {
+        rc = c2q_dslash_eo(tmp2, g, res, C2Q_ODD, kappa);
+        if (!rc) rc = c2q_tm_sitediagonal(tmp1, tmp2, mubar, C2Q_DIAG_M_TM_INVERSE);
+        if (!rc) rc = c2q_tm_sitediagonal(tmp2, src_odd, mubar, C2Q_DIAG_M_TM_INVERSE);
+        if (!rc) rc = c2q_saxpy(tmp1, -1, 0, tmp1, tmp2);
+        if (!rc) rc = c2q_sax(tmp1, -1, 0, tmp1);
+    } else {
+        rc = c2q_dslash_eo(tmp1, g, res, C2Q_ODD, kappa);
+        if (!rc) rc = c2q_saxpy(tmp1, -1, 0, tmp1, src_odd);
+        if (!rc) rc = c2q_sax(tmp1, -1, 0, tmp1);
+    }
+    if (rc) return rc;
+    rc = c2q_convert_from_eoprec(result, tmp1, res);
+    return rc ? rc : conv;
+}
+
+}  // extern "C"

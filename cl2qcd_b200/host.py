@@ -1,0 +1,423 @@
+"""Python mirror of the reference's host surface for the eo tm-Wilson inverter path.
+
+Names, argument meaning and error behaviour follow CL2QCD:
+
+* ``System``            -- hardware::System (hardware/system.cpp:117-200): one CUDA context/stream.
+* ``Lattice``           -- nSpace/nTime/thetaFermion*/chemicalPotential* input parameters.
+* ``Gaugefield``        -- physics::lattices::Gaugefield (physics/lattices/gaugefield.hpp:44-139).
+* ``Spinorfield_eo``    -- physics::lattices::Spinorfield_eo (physics/lattices/spinorfield_eo.hpp:48-305),
+  with the free BLAS functions saxpy (y - a x), sax, saxsbypz, scalar_product,
+  squarenorm, saxpy_AND_squarenorm, saxpy_AND_gamma5_eo, copyData,
+  convert_to_eoprec, convert_from_eoprec.
+* ``dslash``, ``M_tm_*sitediagonal*`` -- physics::fermionmatrix explicit ops
+  (physics/fermionmatrix/fermionmatrix.hpp:46-61).
+* ``Aee``, ``Aee_minus``, ``Qplus_eo``, ``Qminus_eo``, ``QplusQminus_eo`` -- the eo
+  fermion matrices (fermionmatrix.hpp:194-310), called as ``A(out, gf, in, params)``.
+* ``cg``, ``bicgstab`` -- physics::algorithms::solvers (cg.hpp:41-56, bicgstab.hpp:42-57):
+  return the iteration count, raise ``SolverStuck`` / ``SolverDidNotSolve``
+  (physics/algorithms/solvers/exceptions.hpp:35-62).
+* ``perform_inversion`` -- physics::algorithms::perform_inversion, eo branch (inversion.cpp:44-242).
+
+Everything runs in the CUDA library; nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+class SolverException(RuntimeError):
+    """physics::algorithms::solvers::SolverException"""
+
+    def __init__(self, iterations, msg=""):
+        super().__init__(msg or self.__class__.__name__)
+        self.iterations = iterations
+
+
+class SolverStuck(SolverException):
+    pass
+
+
+class SolverDidNotSolve(SolverException):
+    pass
+
+
+class InvalidParameters(ValueError):
+    """Invalid_Parameters / std::invalid_argument of the reference."""
+
+
+def _check(rc, ctx=None, lib=None):
+    if rc >= 0:
+        return rc
+    msg = ""
+    if ctx is not None and lib is not None:
+        msg = (lib.c2q_last_error(ctx) or b"").decode()
+    if rc == L.BAD_ARG:
+        raise InvalidParameters(msg)
+    raise L.C2QError(rc, msg)
+
+
+class System:
+    """One device context (hardware::System with one device)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.lib = L.load()
+        h = C.c_void_p()
+        rc = self.lib.c2q_ctx_create(C.byref(h), device, C.c_void_p(stream) if stream else None)
+        if rc != 0:
+            raise L.C2QError(rc, "c2q_ctx_create failed (no CUDA device?)")
+        self.h = h
+
+    def synchronize(self):
+        _check(self.lib.c2q_ctx_synchronize(self.h), self.h, self.lib)
+
+    @property
+    def launch_count(self) -> int:
+        return self.lib.c2q_ctx_launch_count(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.c2q_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass(frozen=True)
+class Lattice:
+    """nSpace, nTime, thetaFermionTemporal/Spatial (units of pi), chemical potential."""
+
+    ns: int
+    nt: int
+    theta_t: float = 0.0
+    theta_s: float = 0.0
+    cp_re: float | None = None
+    cp_im: float | None = None
+
+    def c(self) -> L.CLattice:
+        return L.CLattice(self.ns, self.nt, self.theta_t, self.theta_s, int(self.cp_re is not None),
+                          int(self.cp_im is not None), self.cp_re or 0.0, self.cp_im or 0.0)
+
+    @property
+    def vol(self):
+        return self.ns ** 3 * self.nt
+
+    @property
+    def seo(self):
+        return self.vol // 2
+
+
+@dataclass
+class AdditionalParameters:
+    """physics::AdditionalParameters: kappa and mubar = 2 kappa mu (meta/util.cpp:56-59)."""
+
+    kappa: float
+    mubar: float = 0.0
+
+    @classmethod
+    def from_mu(cls, kappa, mu):
+        return cls(kappa, 2.0 * kappa * mu)
+
+
+class Gaugefield:
+    def __init__(self, system: System, lattice: Lattice, aos: np.ndarray | None = None):
+        self.system, self.lattice = system, lattice
+        lib = system.lib
+        h = C.c_void_p()
+        lc = lattice.c()
+        _check(lib.c2q_gauge_create(system.h, C.byref(lc), C.byref(h)), system.h, lib)
+        self.h = h
+        if aos is not None:
+            self.upload(aos)
+
+    def upload(self, aos):
+        aos = np.ascontiguousarray(aos, dtype=np.float64)
+        assert aos.size == 4 * self.lattice.vol * 18
+        _check(self.system.lib.c2q_gauge_upload(self.h, aos.reshape(-1)), self.system.h, self.system.lib)
+
+    def download(self):
+        out = np.zeros(4 * self.lattice.vol * 18)
+        _check(self.system.lib.c2q_gauge_download(self.h, out), self.system.h, self.system.lib)
+        return out.reshape(4 * self.lattice.vol, 18)
+
+    @property
+    def device_bytes(self):
+        return self.system.lib.c2q_gauge_device_bytes(self.h)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.system.lib.c2q_gauge_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class Spinorfield_eo:
+    def __init__(self, system: System, lattice: Lattice, aos: np.ndarray | None = None):
+        self.system, self.lattice = system, lattice
+        lib = system.lib
+        h = C.c_void_p()
+        lc = lattice.c()
+        _check(lib.c2q_spinor_eo_create(system.h, C.byref(lc), C.byref(h)), system.h, lib)
+        self.h = h
+        if aos is not None:
+            self.load(aos)
+
+    # Spinor::load / dump
+    def load(self, aos):
+        aos = np.ascontiguousarray(aos, dtype=np.float64).reshape(-1)
+        assert aos.size == self.lattice.seo * 24
+        _check(self.system.lib.c2q_spinor_eo_upload(self.h, aos), self.system.h, self.system.lib)
+
+    def dump(self):
+        out = np.zeros(self.lattice.seo * 24)
+        _check(self.system.lib.c2q_spinor_eo_download(self.h, out), self.system.h, self.system.lib)
+        return out.reshape(self.lattice.seo, 24)
+
+    def zero(self):
+        _check(self.system.lib.c2q_spinor_eo_zero(self.h), self.system.h, self.system.lib)
+
+    def cold(self):
+        _check(self.system.lib.c2q_spinor_eo_cold(self.h), self.system.h, self.system.lib)
+
+    def gamma5(self):
+        _check(self.system.lib.c2q_gamma5_eo(self.h), self.system.h, self.system.lib)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.system.lib.c2q_spinor_eo_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def _sys(f):
+    return f.system
+
+
+def _c(rc, f):
+    return _check(rc, f.system.h, f.system.lib)
+
+
+# ---------------- eo BLAS (physics/lattices/spinorfield_eo.hpp) ----------------
+def saxpy(out, alpha, x, y):
+    """out = y - alpha x"""
+    a = complex(alpha)
+    _c(out.system.lib.c2q_saxpy(out.h, a.real, a.imag, x.h, y.h), out)
+
+
+def saxpy_AND_gamma5_eo(out, alpha, x, y):
+    a = complex(alpha)
+    _c(out.system.lib.c2q_saxpy_AND_gamma5_eo(out.h, a.real, a.imag, x.h, y.h), out)
+
+
+def sax(out, alpha, x):
+    a = complex(alpha)
+    _c(out.system.lib.c2q_sax(out.h, a.real, a.imag, x.h), out)
+
+
+def saxsbypz(out, alpha, x, beta, y, z):
+    a, b = complex(alpha), complex(beta)
+    _c(out.system.lib.c2q_saxsbypz(out.h, a.real, a.imag, x.h, b.real, b.imag, y.h, z.h), out)
+
+
+def copyData(to, frm):
+    _c(to.system.lib.c2q_copyData(to.h, frm.h), to)
+
+
+def scalar_product(x, y) -> complex:
+    re, im = C.c_double(), C.c_double()
+    _c(x.system.lib.c2q_scalar_product(x.h, y.h, C.byref(re), C.byref(im)), x)
+    return complex(re.value, im.value)
+
+
+def squarenorm(x) -> float:
+    r = C.c_double()
+    _c(x.system.lib.c2q_squarenorm(x.h, C.byref(r)), x)
+    return r.value
+
+
+def saxpy_AND_squarenorm(out, alpha, x, y) -> float:
+    a = complex(alpha)
+    r = C.c_double()
+    _c(out.system.lib.c2q_saxpy_AND_squarenorm(out.h, a.real, a.imag, x.h, y.h, C.byref(r)), out)
+    return r.value
+
+
+def convert_to_eoprec(even, odd, full):
+    full = np.ascontiguousarray(full, dtype=np.float64).reshape(-1)
+    _c(even.system.lib.c2q_convert_to_eoprec(even.h, odd.h, full), even)
+
+
+def convert_from_eoprec(even, odd) -> np.ndarray:
+    out = np.zeros(even.lattice.vol * 24)
+    _c(even.system.lib.c2q_convert_from_eoprec(out, even.h, odd.h), even)
+    return out.reshape(even.lattice.vol, 24)
+
+
+# ---------------- explicit fermion ops (physics/fermionmatrix/explicit.cpp) ----------------
+EVEN, ODD = L.EVEN, L.ODD
+
+
+def dslash(out, gf, in_, evenodd, kappa):
+    _c(out.system.lib.c2q_dslash_eo(out.h, gf.h, in_.h, evenodd, kappa), out)
+
+
+def dslash_AND_M_tm_inverse_sitediagonal(out, gf, in_, evenodd, kappa, mubar, minus=False):
+    _c(out.system.lib.c2q_dslash_AND_M_tm_inverse_sitediagonal_eo(out.h, gf.h, in_.h, evenodd, kappa, mubar,
+                                                                  int(minus)), out)
+
+
+def _diag(which):
+    def f(out, in_, mubar):
+        _c(out.system.lib.c2q_tm_sitediagonal(out.h, in_.h, mubar, which), out)
+
+    return f
+
+
+M_tm_sitediagonal = _diag(L.DIAG_M_TM)
+M_tm_inverse_sitediagonal = _diag(L.DIAG_M_TM_INVERSE)
+M_tm_sitediagonal_minus = _diag(L.DIAG_M_TM_MINUS)
+M_tm_inverse_sitediagonal_minus = _diag(L.DIAG_M_TM_INVERSE_MINUS)
+M_tm_sitediagonal_AND_gamma5_eo = _diag(L.DIAG_M_TM_AND_GAMMA5)
+M_tm_sitediagonal_minus_AND_gamma5_eo = _diag(L.DIAG_M_TM_MINUS_AND_GAMMA5)
+
+
+# ---------------- eo fermion matrices ----------------
+class Fermionmatrix_eo:
+    OP = None
+
+    def __init__(self, action: str = "twistedmass", merged: bool = False):
+        act = action.lower()
+        if act not in ("wilson", "twistedmass"):
+            raise InvalidParameters("Unkown fermion action! (wilson or twistedmass)")
+        self.action = L.WILSON if act == "wilson" else L.TWISTEDMASS
+        self.merged = merged
+
+    def __call__(self, out, gf, in_, params: AdditionalParameters):
+        _c(out.system.lib.c2q_apply_eo(self.OP, out.h, gf.h, in_.h, params.kappa, params.mubar, self.action,
+                                       int(self.merged)), out)
+
+
+class Aee(Fermionmatrix_eo):
+    OP = L.OP_AEE
+
+
+class Aee_minus(Fermionmatrix_eo):
+    OP = L.OP_AEE_MINUS
+
+
+class Aee_AND_gamma5_eo(Fermionmatrix_eo):
+    OP = L.OP_AEE_AND_GAMMA5_EO
+
+
+class Aee_minus_AND_gamma5_eo(Fermionmatrix_eo):
+    OP = L.OP_AEE_MINUS_AND_GAMMA5_EO
+
+
+class Qplus_eo(Fermionmatrix_eo):
+    OP = L.OP_QPLUS_EO
+
+
+class Qminus_eo(Fermionmatrix_eo):
+    OP = L.OP_QMINUS_EO
+
+
+class QplusQminus_eo(Fermionmatrix_eo):
+    OP = L.OP_QPLUSQMINUS_EO
+
+
+# ---------------- solvers ----------------
+@dataclass
+class SolverParameters:
+    """SolversParametersInterface (defaults of meta/parametersSolver.cpp:74-107) plus the
+    precision/reliable-update/rel_tol extensions of this build."""
+
+    solver: str = "bicgstab"
+    prec: float = 1e-23
+    rel_tol: float = 0.0
+    cgmax: int = 1000
+    iter_refresh: int = 100
+    resid_check_every: int = 10
+    min_iter: int = 0
+    precision: int = 64
+    reliable_delta: float = 0.1
+    use_rec12: bool = False
+    use_graph: bool = False
+
+    def c(self) -> L.CSolverParams:
+        s = {"cg": L.SOLVER_CG, "bicgstab": L.SOLVER_BICGSTAB, "bicgstab_save": L.SOLVER_BICGSTAB_SAVE}
+        if self.solver not in s:
+            raise InvalidParameters(f"unknown solver {self.solver}")
+        return L.CSolverParams(s[self.solver], self.prec, self.rel_tol, self.cgmax, self.iter_refresh,
+                               self.resid_check_every, self.min_iter, self.precision, self.reliable_delta,
+                               int(self.use_rec12), int(self.use_graph))
+
+
+def _solve(fn, x, A, gf, b, params, add, report):
+    lib = x.system.lib
+    p = params.c()
+    rep = L.CSolveReport()
+    rc = fn(x.h, A.OP, gf.h, b.h, add.kappa, add.mubar, A.action, C.byref(p), C.byref(rep))
+    if report is not None:
+        report.update(rep.as_dict())
+    if rc == L.SOLVER_STUCK:
+        raise SolverStuck(rep.iterations, (lib.c2q_last_error(x.system.h) or b"").decode())
+    if rc == L.DID_NOT_SOLVE:
+        raise SolverDidNotSolve(rep.iterations, (lib.c2q_last_error(x.system.h) or b"").decode())
+    return _check(rc, x.system.h, lib)
+
+
+def cg(x, A, gf, b, params: SolverParameters, add: AdditionalParameters, report: dict | None = None) -> int:
+    return _solve(x.system.lib.c2q_cg, x, A, gf, b, params, add, report)
+
+
+def bicgstab(x, A, gf, b, params: SolverParameters, add: AdditionalParameters, report: dict | None = None) -> int:
+    return _solve(x.system.lib.c2q_bicgstab, x, A, gf, b, params, add, report)
+
+
+def perform_inversion(system: System, gf: Gaugefield, source: np.ndarray, params: SolverParameters,
+                      add: AdditionalParameters, action: str = "twistedmass", report: dict | None = None):
+    """One source of perform_inversion (eo); returns the full result field (reference sign convention)."""
+    lib = system.lib
+    src = np.ascontiguousarray(source, dtype=np.float64).reshape(-1)
+    out = np.zeros_like(src)
+    p = params.c()
+    rep = L.CSolveReport()
+    act = L.WILSON if action.lower() == "wilson" else L.TWISTEDMASS
+    rc = lib.c2q_perform_inversion_eo(system.h, out, gf.h, src, add.kappa, add.mubar, act, C.byref(p),
+                                      C.byref(rep))
+    if report is not None:
+        report.update(rep.as_dict())
+    if rc == L.SOLVER_STUCK:
+        raise SolverStuck(rep.iterations)
+    if rc == L.DID_NOT_SOLVE:
+        raise SolverDidNotSolve(rep.iterations)
+    _check(rc, system.h, lib)
+    return out.reshape(gf.lattice.vol, 24), rc
+
+
+# ---------------- inputs ----------------
+def generate_gaugefield(lattice: Lattice, eps: float, seed: int) -> np.ndarray:
+    """U = exp(i eps H), reunitarised (host, library code)."""
+    lib = L.load()
+    out = np.zeros(4 * lattice.vol * 18)
+    _check(lib.c2q_gauge_generate(out, lattice.ns, lattice.nt, eps, seed))
+    return out.reshape(4 * lattice.vol, 18)
+
+
+def generate_source(n_sites: int, kind: str, seed: int) -> np.ndarray:
+    lib = L.load()
+    out = np.zeros(n_sites * 24)
+    _check(lib.c2q_source_generate(out, n_sites, {"z2": 0, "gaussian": 1}[kind], seed))
+    return out.reshape(n_sites, 24)

@@ -1,0 +1,251 @@
+/*
+ * cl2qcd_b200.h -- C ABI of the B200-native twisted-mass Wilson even-odd
+ * inverter hot path (CL2QCD's dslash_eo / M_tm sitediagonal / eo BLAS /
+ * CG / BiCGStab / eo inversion), implemented in hand-written sm_100a CUDA.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, integer status codes.
+ * Every entry point names the reference interface it replaces (file:line in
+ * the CL2QCD tree).
+ *
+ * Host data formats are the reference's:
+ *   eo spinor field : double[Seo][24], eo index order (site/2), each spinor
+ *                     [spin 0..3][colour 0..2][re, im]
+ *                     (common_header_files/types_fermions.hpp:31-55,
+ *                      hardware/buffers/spinor.cpp:83-106);
+ *   full spinor     : double[V][24] in site order x + NS y + NS^2 z + NS^3 t
+ *                     (geometry/index.cpp:46-70);
+ *   gauge field     : double[4 V][18], Matrixsu3 at link mu + 4*site with
+ *                     TDIR = 0, XDIR = 1, YDIR = 2, ZDIR = 3, row-major
+ *                     (re, im) (hardware/code/gaugefield.cpp:533,
+ *                      geometry/latticeExtents.hpp:28).
+ *
+ * Threading: one CUDA stream per context; calls on a context are ordered on
+ * that stream.  Calls that return host scalars or reports synchronise the
+ * stream.  A context is thread-compatible (one host thread at a time), not
+ * thread-safe.  Different contexts may be used from different threads.
+ */
+#ifndef CL2QCD_B200_H
+#define CL2QCD_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define C2Q_EXPORT __attribute__((visibility("default")))
+#else
+#define C2Q_EXPORT
+#endif
+
+/* ---- status codes (the C++ mirror maps them back to the reference's
+ *      exception types, physics/algorithms/solvers/exceptions.hpp:35-62) ---- */
+#define C2Q_OK 0
+#define C2Q_SOLVER_STUCK -1   /* SolverStuck: NaN residual or |rho| < 1e-25 */
+#define C2Q_DID_NOT_SOLVE -2  /* SolverDidNotSolve: iteration limit reached */
+#define C2Q_TIMEOUT -3
+#define C2Q_OOM -4
+#define C2Q_BAD_ARG -5        /* Invalid_Parameters / std::invalid_argument */
+#define C2Q_CUDA_ERROR -6
+#define C2Q_NO_DEVICE -7
+
+/* evenodd argument of c2q_dslash_eo, with the reference's meaning
+ * (common_header_files/globaldefs.hpp:38-39; ocl_kernel/fermionmatrix_eo_dslash.cl:50-58):
+ * ODD writes the sites with x+y+z+t even, EVEN writes the odd sites. */
+#define C2Q_EVEN 0
+#define C2Q_ODD 1
+
+/* fermion actions (common_header_files/types.hpp:198, the subset on this path) */
+#define C2Q_ACTION_WILSON 1
+#define C2Q_ACTION_TWISTEDMASS 3
+
+/* eo fermion matrices (physics/fermionmatrix/fermionmatrix.hpp:194-310) */
+#define C2Q_OP_AEE 0
+#define C2Q_OP_AEE_MINUS 1
+#define C2Q_OP_QPLUS_EO 2
+#define C2Q_OP_QMINUS_EO 3
+#define C2Q_OP_QPLUSQMINUS_EO 4
+#define C2Q_OP_AEE_AND_GAMMA5_EO 5
+#define C2Q_OP_AEE_MINUS_AND_GAMMA5_EO 6
+
+/* site-diagonal tm factors (physics/fermionmatrix/fermionmatrix.hpp:50-57;
+ * ocl_kernel/fermionmatrix_eo_m.cl:22-109, fermionmatrix_eo_m_merged.cl:22-64) */
+#define C2Q_DIAG_M_TM 0              /* M_tm_sitediagonal:               1 + i mubar g5 */
+#define C2Q_DIAG_M_TM_INVERSE 1      /* M_tm_inverse_sitediagonal:       (1 - i mubar g5)/(1+mubar^2) */
+#define C2Q_DIAG_M_TM_MINUS 2        /* M_tm_sitediagonal_minus:         1 - i mubar g5 */
+#define C2Q_DIAG_M_TM_INVERSE_MINUS 3/* M_tm_inverse_sitediagonal_minus: (1 + i mubar g5)/(1+mubar^2) */
+#define C2Q_DIAG_M_TM_AND_GAMMA5 4   /* M_tm_sitediagonal_AND_gamma5_eo */
+#define C2Q_DIAG_M_TM_MINUS_AND_GAMMA5 5
+
+/* solvers (common_header_files/types.hpp:199 common::solver) */
+#define C2Q_SOLVER_CG 1
+#define C2Q_SOLVER_BICGSTAB 2
+#define C2Q_SOLVER_BICGSTAB_SAVE 3
+
+/* inner precision of the Krylov iteration */
+#define C2Q_PREC_FP64 64   /* plain FP64, the reference's arithmetic */
+#define C2Q_PREC_FP32 32   /* FP32 inner solve inside FP64 reliable updates */
+#define C2Q_PREC_FP16 16   /* FP16 fixed-point spinors (per-site norm) + FP32 arithmetic, FP64 reliable updates */
+
+typedef struct c2q_ctx c2q_ctx;
+typedef struct c2q_gauge c2q_gauge;
+typedef struct c2q_spinor_eo c2q_spinor_eo;
+
+/* Lattice and boundary conditions.  Replaces the lattice/BC parameters the
+ * reference bakes into its kernels as build options
+ * (hardware/code/opencl_module.cpp:61-224; meta/parametersFermion.cpp:106-150):
+ * nSpace, nTime, thetaFermionTemporal/Spatial (units of pi; phase theta*pi/N
+ * on every hop), useChemicalPotentialRe/Im and chemicalPotentialRe/Im. */
+typedef struct {
+    int ns, nt;            /* both even */
+    double theta_t, theta_s;
+    int use_cp_re, use_cp_im;
+    double cp_re, cp_im;
+} c2q_lattice;
+
+/* Solver parameters.  Replaces SolversParametersInterface
+ * (physics/algorithms/algorithmsInterfaces.hpp:28-37; defaults of
+ * meta/parametersSolver.cpp:74-107). */
+typedef struct {
+    int solver;               /* C2Q_SOLVER_* (solver) */
+    double prec;              /* solverPrecision: stop when |r|^2 < prec (absolute, reference semantics); <= 0 disables */
+    double rel_tol;           /* additionally stop when ||b - A x|| / ||b|| <= rel_tol (true residual); <= 0 disables */
+    int cgmax;                /* solverMaxIterations */
+    int iter_refresh;         /* solverRestartEvery */
+    int resid_check_every;    /* solverResiduumCheckEvery (CG) */
+    int min_iter;             /* solverMinIterations (CG) */
+    int precision;            /* C2Q_PREC_*: inner arithmetic */
+    double reliable_delta;    /* mixed precision: reliable update when |r_inner| < delta * max|r| since the last one */
+    int use_rec12;            /* inner operator uses 12-real links */
+    int use_graph;            /* capture the iterations between residual checks in a CUDA graph */
+} c2q_solver_params;
+
+/* What a solve reports (replaces the reference's log lines,
+ * physics/algorithms/solvers/cg.cpp:195-275). */
+typedef struct {
+    int status;               /* >= 0 iterations, else C2Q_* status */
+    int iterations;           /* inner Krylov iterations */
+    int reliable_updates;     /* FP64 residual recomputations (mixed precision) */
+    double resid_sq;          /* last iterated |r|^2 */
+    double true_resid_rel;    /* ||b - A x|| / ||b|| recomputed in FP64 at the end */
+    double seconds;           /* device time of the solve (CUDA events) */
+    double dslash_applications; /* dslash launches (each = one parity sweep over the lattice) */
+} c2q_solve_report;
+
+/* ---------------- context ---------------- */
+/* Creates a context on `device`.  `cuda_stream` (a cudaStream_t) is borrowed
+ * if non-NULL, else the context creates its own.  Replaces hardware::System /
+ * hardware::Device (hardware/system.cpp:117-200, hardware/device.cpp:79). */
+C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream);
+C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx);
+C2Q_EXPORT const char* c2q_last_error(const c2q_ctx* ctx);
+C2Q_EXPORT int c2q_ctx_synchronize(c2q_ctx* ctx);
+/* Kernels this library launched on the context since creation (all of them are this library's own). */
+C2Q_EXPORT long long c2q_ctx_launch_count(const c2q_ctx* ctx);
+
+/* ---------------- gauge field ---------------- */
+/* Gaugefield device layout + import (physics/lattices/gaugefield.hpp:44-139;
+ * hardware/code/gaugefield.cpp:533 importGaugefield).  `aos` is Matrixsu3[4V]. */
+C2Q_EXPORT int c2q_gauge_create(c2q_ctx* ctx, const c2q_lattice* lat, c2q_gauge** out);
+C2Q_EXPORT int c2q_gauge_upload(c2q_gauge* g, const double* aos);
+C2Q_EXPORT int c2q_gauge_download(const c2q_gauge* g, double* aos);
+C2Q_EXPORT int c2q_gauge_destroy(c2q_gauge* g);
+/* Device bytes held by the gauge object (all precisions built so far). */
+C2Q_EXPORT size_t c2q_gauge_device_bytes(const c2q_gauge* g);
+
+/* ---------------- eo spinor fields (FP64) ---------------- */
+/* physics::lattices::Spinorfield_eo (physics/lattices/spinorfield_eo.hpp:48-305). */
+C2Q_EXPORT int c2q_spinor_eo_create(c2q_ctx* ctx, const c2q_lattice* lat, c2q_spinor_eo** out);
+C2Q_EXPORT int c2q_spinor_eo_destroy(c2q_spinor_eo* f);
+/* Spinor::load / dump (hardware/buffers/spinor.cpp:83-106): spinor[Seo] in eo index order. */
+C2Q_EXPORT int c2q_spinor_eo_upload(c2q_spinor_eo* f, const double* aos);
+C2Q_EXPORT int c2q_spinor_eo_download(const c2q_spinor_eo* f, double* aos);
+/* Spinorfield_eo::zero / cold (physics/lattices/spinorfield_eo.cpp:147-165) */
+C2Q_EXPORT int c2q_spinor_eo_zero(c2q_spinor_eo* f);
+C2Q_EXPORT int c2q_spinor_eo_cold(c2q_spinor_eo* f);
+/* convert_to_eoprec / convert_from_eoprec (physics/lattices/spinorfield_eo.cpp:372-410):
+ * `full` is a host spinor[V]; `even` gets the sites with x+y+z+t even. */
+C2Q_EXPORT int c2q_convert_to_eoprec(c2q_spinor_eo* even, c2q_spinor_eo* odd, const double* full);
+C2Q_EXPORT int c2q_convert_from_eoprec(double* full, const c2q_spinor_eo* even, const c2q_spinor_eo* odd);
+
+/* ---------------- explicit fermion operations ---------------- */
+/* physics::fermionmatrix::dslash (physics/fermionmatrix/explicit.cpp:185-222) */
+C2Q_EXPORT int c2q_dslash_eo(c2q_spinor_eo* out, const c2q_gauge* g, const c2q_spinor_eo* in, int evenodd,
+                             double kappa);
+/* Fermions::dslash_AND_M_tm_inverse_sitediagonal(_minus)_eo_device (hardware/code/fermions.cpp:550-623) */
+C2Q_EXPORT int c2q_dslash_AND_M_tm_inverse_sitediagonal_eo(c2q_spinor_eo* out, const c2q_gauge* g,
+                                                           const c2q_spinor_eo* in, int evenodd, double kappa,
+                                                           double mubar, int minus);
+/* M_tm_(inverse_)sitediagonal(_minus) (physics/fermionmatrix/explicit.cpp:88-183) and the merged
+ * M_tm_sitediagonal(_minus)_AND_gamma5_eo (hardware/code/fermions.cpp): `which` = C2Q_DIAG_* */
+C2Q_EXPORT int c2q_tm_sitediagonal(c2q_spinor_eo* out, const c2q_spinor_eo* in, double mubar, int which);
+/* Spinorfield_eo::gamma5 (physics/lattices/spinorfield_eo.cpp:412-418) */
+C2Q_EXPORT int c2q_gamma5_eo(c2q_spinor_eo* inout);
+
+/* Fermionmatrix_eo::operator() (physics/fermionmatrix/fermionmatrix.hpp:121-136,
+ * fermionmatrix.cpp:224-664): out = A(in) for op = C2Q_OP_*, action = C2Q_ACTION_*.
+ * `merged` = useKernelMergingFermionMatrix (fermionmatrix.cpp:596). */
+C2Q_EXPORT int c2q_apply_eo(int op, c2q_spinor_eo* out, const c2q_gauge* g, const c2q_spinor_eo* in, double kappa,
+                            double mubar, int action, int merged);
+
+/* ---------------- eo BLAS (physics/lattices/spinorfield_eo.hpp:148-305) ---------------- */
+C2Q_EXPORT int c2q_saxpy(c2q_spinor_eo* out, double alpha_re, double alpha_im, const c2q_spinor_eo* x,
+                         const c2q_spinor_eo* y);                         /* out = y - alpha x */
+C2Q_EXPORT int c2q_saxpy_AND_gamma5_eo(c2q_spinor_eo* out, double alpha_re, double alpha_im,
+                                       const c2q_spinor_eo* x, const c2q_spinor_eo* y); /* out = g5 (y - alpha x) */
+C2Q_EXPORT int c2q_sax(c2q_spinor_eo* out, double alpha_re, double alpha_im, const c2q_spinor_eo* x);
+C2Q_EXPORT int c2q_saxsbypz(c2q_spinor_eo* out, double alpha_re, double alpha_im, const c2q_spinor_eo* x,
+                            double beta_re, double beta_im, const c2q_spinor_eo* y, const c2q_spinor_eo* z);
+C2Q_EXPORT int c2q_copyData(c2q_spinor_eo* to, const c2q_spinor_eo* from);
+C2Q_EXPORT int c2q_scalar_product(const c2q_spinor_eo* x, const c2q_spinor_eo* y, double* re, double* im);
+C2Q_EXPORT int c2q_squarenorm(const c2q_spinor_eo* x, double* result);
+C2Q_EXPORT int c2q_saxpy_AND_squarenorm(c2q_spinor_eo* out, double alpha_re, double alpha_im,
+                                        const c2q_spinor_eo* x, const c2q_spinor_eo* y, double* squarenorm);
+
+/* ---------------- solvers ---------------- */
+C2Q_EXPORT void c2q_solver_params_default(c2q_solver_params* p);
+/* solvers::cg (physics/algorithms/solvers/cg.hpp:41-56, cg.cpp:158-170, 277-400):
+ * solves A x = b for op (normally C2Q_OP_QPLUSQMINUS_EO), x holds the start
+ * vector on entry.  Returns iterations (>= 0) or C2Q_SOLVER_STUCK /
+ * C2Q_DID_NOT_SOLVE / other status. */
+C2Q_EXPORT int c2q_cg(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
+                      double mubar, int action, const c2q_solver_params* p, c2q_solve_report* report);
+/* solvers::bicgstab (physics/algorithms/solvers/bicgstab.hpp:42-57, bicgstab.cpp:384-733);
+ * p->solver selects the fast (C2Q_SOLVER_BICGSTAB) or save (C2Q_SOLVER_BICGSTAB_SAVE) variant. */
+C2Q_EXPORT int c2q_bicgstab(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
+                            double mubar, int action, const c2q_solver_params* p, c2q_solve_report* report);
+/* Multi-right-hand-side CG on one operator: x[k], b[k] for k < nrhs (each
+ * right-hand side converges on its own; the dslash reads each link once per
+ * batch).  Same semantics per right-hand side as c2q_cg. */
+C2Q_EXPORT int c2q_cg_multi(c2q_spinor_eo* const* x, int op, const c2q_gauge* g, const c2q_spinor_eo* const* b,
+                            int nrhs, double kappa, double mubar, int action, const c2q_solver_params* p,
+                            c2q_solve_report* reports);
+
+/* physics::algorithms::perform_inversion, eo branch of invert_M_nf2_upperflavour
+ * (physics/algorithms/inversion.cpp:44-76, 78-242), one source: `source` and
+ * `result` are host full fields spinor[V].  Reproduces the reference
+ * literally, including its parity-role swap (inversion.cpp:141-149) and sign
+ * conventions (inversion.cpp:165-169, 204-221), which make the returned
+ * field equal to -M^{-1} source. */
+C2Q_EXPORT int c2q_perform_inversion_eo(c2q_ctx* ctx, double* result, const c2q_gauge* g, const double* source,
+                                        double kappa, double mubar, int action, const c2q_solver_params* p,
+                                        c2q_solve_report* report);
+
+/* ---------------- inputs ---------------- */
+/* Seeded synthetic gauge field U = exp(i eps H), H traceless Hermitian with
+ * N(0,1) entries, reunitarised in FP64 (host computation, no GPU needed).
+ * Writes Matrixsu3[4V] in the reference's AoS layout. */
+C2Q_EXPORT int c2q_gauge_generate(double* aos, int ns, int nt, double eps, unsigned long long seed);
+/* Seeded sources into host arrays of n_sites spinors:
+ * kind 0 = Z2 noise ((+-1 +-i)/sqrt 2 per component), 1 = Gaussian (complex N(0,1) per component). */
+C2Q_EXPORT int c2q_source_generate(double* aos, size_t n_sites, int kind, unsigned long long seed);
+
+/* Library version string. */
+C2Q_EXPORT const char* c2q_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

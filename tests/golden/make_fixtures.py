@@ -1,0 +1,110 @@
+"""Regenerate the golden fixtures of tests/golden/ (run in a container that has the
+reference tree and the oracle built; the fixtures themselves are committed).
+
+1. reference_kats.json -- the known-answer values the reference's own tests
+   hold for this path, extracted verbatim (by regex) from its test sources:
+   * physics/fermionmatrix/fermionmatrix_test.cpp: Aee, Aee_minus, Qplus_eo,
+     Qminus_eo, QplusQminus_eo (squarenorm after one and two applications,
+     cold 4^3x16 block, seeds 5..9);
+   * physics/fermionmatrix/explicit_test.cpp: dslash (seed 13) and the four
+     M_tm_*sitediagonal* cases (seeds 5, 7, 9, 11);
+   * hardware/code/fermions_test.cpp: the closed form of the dslash_eo
+     kernel test in theta and the chemical potential, and the
+     M_tm_sitediagonal family per-site constants.
+2. ref_outputs.npz -- outputs of the reference's own kernels (oracle/_ref/
+   libc2q_ref.so, compiled from the reference sources) on small seeded
+   inputs, used to pin the restated oracle and the CUDA path.
+
+Usage:  python tests/golden/make_fixtures.py [/path/to/reference]
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+
+def _floats(s):
+    return [float(x) for x in re.findall(r"[-+]?\d*\.\d+(?:[eE][-+]?\d+)?|[-+]?\d+\.(?:[eE][-+]?\d+)?", s)]
+
+
+def extract_kats(ref: str) -> dict:
+    out = {"source": "reference test sources, values copied by regex", "fermionmatrix_eo": {}, "explicit": {}}
+    fm = open(os.path.join(ref, "physics/fermionmatrix/fermionmatrix_test.cpp")).read()
+    for m in re.finditer(r"BOOST_AUTO_TEST_CASE\((\w+)\)\s*\{\s*const hmc_float refs\[4\] = \{([^}]*)\};\s*"
+                         r"test_fermionmatrix<physics::fermionmatrix::(\w+)>\(refs, (\d+)\);", fm):
+        name, vals, cls, seed = m.group(1), _floats(m.group(2)), m.group(3), int(m.group(4))
+        if cls.endswith("_eo") or cls.startswith("Aee"):
+            out["fermionmatrix_eo"][cls] = {"seed": seed, "refs": vals,
+                                            "where": "physics/fermionmatrix/fermionmatrix_test.cpp"}
+    ex = open(os.path.join(ref, "physics/fermionmatrix/explicit_test.cpp")).read()
+    for m in re.finditer(r"BOOST_AUTO_TEST_CASE\((\w+)\)(.*?)(?=BOOST_AUTO_TEST_CASE|\Z)", ex, re.S):
+        name, body = m.group(1), m.group(2)
+        first = body.split("conf.00200")[0] if "conf.00200" in body else body
+        seeds = re.findall(r"pseudo_randomize<Spinorfield, spinor>\(&src, (\d+)\)", first)
+        refs = re.findall(r"BOOST_CHECK_CLOSE\(squarenorm\(\w+\), ([-+0-9.eE]+), 0\.01\)", first)
+        nt = re.findall(r"--nTime=(\d+)", first)
+        if seeds and refs and ("sitediag" in name or name == "dslash"):
+            out["explicit"][name] = {"seed": int(seeds[0]), "refs": [float(r) for r in refs[:2]],
+                                     "nt": int(nt[0]) if nt else None,
+                                     "where": "physics/fermionmatrix/explicit_test.cpp"}
+    ft = open(os.path.join(ref, "hardware/code/fermions_test.cpp")).read()
+    m = re.search(r"calculateReferenceValuesDslashEvenOdd.*?return ReferenceValues\{(.*?)\};", ft, re.S)
+    coeffs = _floats(m.group(1))
+    out["dslash_eo_closed_form"] = {
+        "coefficients": coeffs[:6],
+        "form": "Seo*(c0*cos(pi thS/NS) + c1*cos(cpi + pi thT/NT)*cosh(cpr) + c2*sin(pi thS/NS) "
+                "+ c3*cosh(cpr)*sin(cpi + pi thT/NT) + c4*cos(cpi + pi thT/NT)*sinh(cpr) "
+                "+ c5*sin(cpi + pi thT/NT)*sinh(cpr)), signs included in the coefficients",
+        "kappa": 0.123456, "fill": "ascendingComplex spinor, nonTrivial gauge",
+        "where": "hardware/code/fermions_test.cpp:106-125",
+    }
+    # signs of the closed form terms as written in the source
+    body = m.group(1)
+    signs = []
+    for term in re.finditer(r"([-+])?\s*([0-9.]+)\s*\*", body):
+        signs.append(-1.0 if term.group(1) == "-" else 1.0)
+    out["dslash_eo_closed_form"]["coefficients"] = [s * abs(c) for s, c in zip(signs, coeffs[:6])]
+    diag = {}
+    for fn in ["mTmSitediagonal", "mTmSitediagonalMinus", "mTmInverseSitediagonal", "mTmInverseSitediagonalMinus"]:
+        mm = re.search(r"calculateReferenceValues_" + fn + r"\(.*?ReferenceValues\{latticeVolume \* ([0-9.]+)\}",
+                       ft, re.S)
+        diag[fn] = float(mm.group(1))
+    out["tm_sitediagonal_per_site"] = {"values": diag, "kappa": 0.123456, "mu": 0.123456,
+                                       "fill": "ascendingComplex", "lattice": [4, 8],
+                                       "where": "hardware/code/fermions_test.cpp:69-104,483-507"}
+    return out
+
+
+def make_ref_outputs(path):
+    import oracle as O
+    R = O.Oracle("reference")
+    data = {}
+    # 4^4, random (drand48) non-unitary gauge and spinor, antiperiodic T and a spatial phase
+    R.set_lattice(4, 4, 1.0, 0.3)
+    g = np.zeros((4 * R.vol, 18))
+    R.lib.c2qo_pseudo_randomize(g, g.size, 3)
+    s = R.pseudo_randomize(R.seo, 4)
+    data["lat4_gauge_seed"] = np.array([3])
+    data["lat4_spinor_seed"] = np.array([4])
+    data["lat4_dslash_even"] = R.dslash_eo(s, g, O.EVEN, 0.15)
+    data["lat4_dslash_odd"] = R.dslash_eo(s, g, O.ODD, 0.15)
+    data["lat4_qpqm"] = R.apply(O.OP_QPQM_EO, s, g, 0.15, 0.03)
+    data["lat4_dslash_tminv_odd"] = R.dslash_tm_inv_eo(s, g, O.ODD, 0.15, 0.03)
+    np.savez_compressed(path, **data)
+
+
+if __name__ == "__main__":
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    kats = extract_kats(ref)
+    with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
+        json.dump(kats, f, indent=1, sort_keys=True)
+    make_ref_outputs(os.path.join(HERE, "ref_outputs.npz"))
+    print("wrote", os.path.join(HERE, "reference_kats.json"), os.path.join(HERE, "ref_outputs.npz"))
