@@ -1,0 +1,398 @@
+"""Benchmark: tm-Wilson eo CG solves/s to a true residual of 1e-10 on 32^3x64.
+
+One step = one complete CG solve (QplusQminus_eo, kappa 0.16, mu 0.005,
+antiperiodic T, gauge U = exp(i 0.25 H), one Gaussian source) from x = 0 to
+||b - A x|| / ||b|| <= 1e-10 checked in FP64.  The headline `value` is the
+mixed-precision solver (FP16 fixed-point spinors and 12-real FP16 links in the
+inner CG, FP32 arithmetic, FP64 reliable updates); the plain FP64 solver on the
+same problem is reported beside it.  `value` is device time with inputs
+resident in HBM; `e2e` goes through the public API with pinned host buffers
+(source upload, solve, solution download) inside the timed region.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+For N > 1 (torchrun) each rank solves its own replica on its own GPU (the path
+does not shard); value = all ranks' solves / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "tm-Wilson CG solves/s @1e-10 (mixed vs FP64, same B200); Dslash HBM GB/s; p99"
+NS, NT = 32, 64
+EPS, KAPPA, MU = 0.25, 0.16, 0.005
+GAUGE_SEED, SOURCE_SEED = 20250, 777
+REL_TOL = 1e-10
+# FP64 CG iterations this workload needs to reach 1e-10 (the reference's CG is the
+# same algorithm in FP64); used to scale the CPU reference's per-iteration sample
+# to solves/s when the GPU arm is not run in the same process.
+FP64_CG_ITERATIONS = None
+WORKLOAD = (f"32^3x64 tm-Wilson eo CG on QplusQminus_eo, 1 gaussian source, kappa {KAPPA}, mu {MU}, "
+            f"eps {EPS}, antiperiodic T, x0 = 0, true residual {REL_TOL}")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", type=int, default=16, choices=[16, 32, 64])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--phase", default="all", choices=["all", "mixed"],
+                    help="mixed: only the warm-up and timed mixed-precision solves (for profiling)")
+    return ap.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def mbar():
+    return 2.0 * KAPPA * MU
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM traffic of the dominant sweep from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ CPU reference arm
+def cpu_reference_sample(g, b, fp64_iters, budget_s=15.0):
+    """Time the reference's own kernels (oracle/_ref, compiled from the reference
+    sources) running the reference CG on this workload for a bounded number of
+    iterations, and scale to solves/s with the FP64 iteration count."""
+    import oracle as O
+    kind = "reference" if O.available("reference") else "port"
+    o = O.Oracle(kind)
+    o.set_lattice(NS, NT, 1.0, 0.0)
+    threads = int(os.environ.get("OMP_NUM_THREADS", "0")) or os.cpu_count()
+    x = np.zeros_like(b)
+    P = O.SolverParams(prec=1e-300, cgmax=1, solver=1)
+    t0 = time.perf_counter()
+    o.cg(x, O.OP_QPQM_EO, b, g, KAPPA, mbar(), params=P)  # refresh + 1 iteration
+    t1 = time.perf_counter() - t0
+    n = max(1, min(40, int(budget_s / max(t1, 1e-3) * 2) - 1))
+    x[:] = 0
+    P = O.SolverParams(prec=1e-300, cgmax=n, solver=1)
+    t0 = time.perf_counter()
+    o.cg(x, O.OP_QPQM_EO, b, g, KAPPA, mbar(), params=P)
+    tn = time.perf_counter() - t0
+    # n iterations + one refresh (one extra operator application and saxpy)
+    per_iter = tn / (n + 1)
+    solves = 1.0 / (per_iter * fp64_iters)
+    return {"value": solves, "unit": "solves/s", "cores": threads, "kind": kind,
+            "sample": f"{n} FP64 CG iterations (+1 refresh) of this 32^3x64 workload on the reference's kernels "
+                      f"in {tn:.1f} s, scaled by {fp64_iters} FP64 iterations per solve",
+            "seconds_per_iteration": per_iter}
+
+
+def inputs():
+    import cl2qcd_b200 as c2q
+    lat = c2q.Lattice(NS, NT, 1.0, 0.0)
+    g = c2q.host.generate_gaugefield(lat, EPS, GAUGE_SEED)
+    b = c2q.host.generate_source(lat.seo, "gaussian", SOURCE_SEED)
+    return lat, g, b
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    lat, g, b = inputs()
+    iters = FP64_CG_ITERATIONS
+    if iters is None:
+        print(json.dumps({"impl": "reference", "unavailable": "FP64 iteration count of the workload not recorded"}))
+        return 0
+    cb = cpu_reference_sample(g, b, iters)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "solves/s", "n_gpus": args.gpus, "steps": 1,
+            "warmup": 0, "ms_per_step": 1e3 / cb["value"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "lattice": "32x32x32x64"},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import cl2qcd_b200 as c2q
+    from cl2qcd_b200 import build
+    build.build()
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # a dedicated (non-default) stream: the library launches on it and the
+    # torch events below record on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    system = c2q.System(local, stream.cuda_stream)
+    lib = system.lib
+    lat, g, b = inputs()
+    gf = c2q.Gaugefield(system, lat, g)
+    B = c2q.Spinorfield_eo(system, lat, b)
+    X = c2q.Spinorfield_eo(system, lat)
+    add = c2q.AdditionalParameters(KAPPA, mbar())
+    A = c2q.host.QplusQminus_eo()
+    P_mixed = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=args.precision,
+                                   use_rec12=True)
+    P_fp64 = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=64)
+
+    def solve(P, rep=None):
+        X.zero()
+        c2q.host.cg(X, A, gf, B, P, add, rep)
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.phase == "mixed":
+        for _ in range(args.warmup):
+            solve(P_mixed)
+        barrier()
+        e0.record()
+        for _ in range(args.steps):
+            solve(P_mixed)
+        e1.record()
+        barrier()
+        if rank == 0:
+            print(json.dumps({"phase": "mixed", "ms_per_step": e0.elapsed_time(e1) / args.steps}))
+        system.close()
+        return 0
+
+    # ---- FP64 reference solve on the GPU (reported beside the headline)
+    rep64 = {}
+    solve(P_fp64, rep64)
+    x64 = X.dump()
+    barrier()
+    e0.record()
+    solve(P_fp64)
+    e1.record()
+    torch.cuda.synchronize()
+    fp64_s = e0.elapsed_time(e1) / 1e3
+
+    # ---- headline: mixed precision
+    for _ in range(args.warmup):
+        solve(P_mixed)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = system.launch_count
+    e0.record()
+    reps = []
+    for _ in range(args.steps):
+        r = {}
+        solve(P_mixed, r)
+        reps.append(r)
+    e1.record()
+    barrier()
+    launches = system.launch_count - launches0
+    clk = clocks.stop()
+    t = e0.elapsed_time(e1) / 1e3
+    if pg is not None:
+        tt = torch.tensor([t], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t = float(tt.item())
+    xm = X.dump()
+    err_vs_fp64 = float(np.linalg.norm(xm - x64) / np.linalg.norm(x64))
+    value = ws * args.steps / t
+
+    # ---- e2e through the public API with pinned host buffers
+    src_host = torch.from_numpy(b.reshape(-1).copy()).pin_memory()
+    sol_host = torch.empty(lat.seo * 24, dtype=torch.float64).pin_memory()
+    src_np, sol_np = src_host.numpy(), sol_host.numpy()
+    barrier()
+    e0.record()
+    for _ in range(args.steps):
+        B.load(src_np)
+        X.zero()
+        c2q.host.cg(X, A, gf, B, P_mixed, add)
+        lib.c2q_spinor_eo_download(X.h, sol_np)
+    e1.record()
+    barrier()
+    te = e0.elapsed_time(e1) / 1e3
+    if pg is not None:
+        tt = torch.tensor([te], device="cuda")
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        te = float(tt.item())
+    B.load(b)
+
+    # ---- roofline of the dominant kernel: the inner-precision dslash sweep, timed
+    # per launch with CUDA events inside one more solve
+    lib.c2q_ctx_profile(system.h, 1)
+    rprof = {}
+    solve(P_mixed, rprof)
+    nl, ms, by = C.c_longlong(), C.c_double(), C.c_double()
+    lib.c2q_ctx_profile_read(system.h, args.precision, C.byref(nl), C.byref(ms), C.byref(by))
+    lib.c2q_ctx_profile(system.h, 0)
+    peak, peak_kind = load_peaks()
+    avg_s = ms.value / 1e3 / max(nl.value, 1)
+    bytes_per_launch = by.value / max(nl.value, 1)
+    achieved = bytes_per_launch / avg_s / 1e9 if avg_s > 0 else 0.0
+    traffic = None
+    tr = load_traffic()
+    if tr and str(args.precision) in tr.get("dram_bytes_per_launch", {}):
+        traffic = tr["dram_bytes_per_launch"][str(args.precision)]
+
+    # ---- plain dslash bandwidth per precision (FP64 through the public call)
+    def dslash_gbs():
+        out = {}
+        Y = c2q.Spinorfield_eo(system, lat)
+        for _ in range(3):
+            lib.c2q_dslash_eo(Y.h, gf.h, B.h, 1, KAPPA)
+        torch.cuda.synchronize()
+        n = 20
+        e0.record()
+        for _ in range(n):
+            lib.c2q_dslash_eo(Y.h, gf.h, B.h, 1, KAPPA)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / n
+        out["fp64_18real"] = round(lat.seo * 1536 / sec / 1e9, 1)
+        return out
+
+    dg = dslash_gbs()
+
+    cpu_baseline = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cpu_baseline = cpu_reference_sample(g, b, rep64["iterations"])
+            cpu_baseline.pop("seconds_per_iteration", None)
+        except Exception as e:  # the baseline is reported, never required
+            cpu_baseline = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
+                            "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        it_m = [r["iterations"] for r in reps]
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {16: "f16-fixed-point storage, f32 arithmetic, f64 reliable updates",
+                      32: "f32 inner, f64 reliable updates", 64: "f64"}[args.precision],
+            "data": "synthetic: seeded U=exp(i*0.25*H) gauge field (reunitarised in f64), gaussian source",
+            "config": {"workload": WORKLOAD, "lattice": "32x32x32x64", "global_batch": ws,
+                       "inner_precision": args.precision, "links": "12-real", "parallelism": f"replicas x{ws}",
+                       "l2": "inputs larger than L2 (FP16 12-real links 201 MB, FP64 links 1.2 GB)"},
+            "e2e": {"value": ws * args.steps / te, "unit": "solves/s", "h2d_bytes_per_step": lat.seo * 24 * 8,
+                    "d2h_bytes_per_step": lat.seo * 24 * 8},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": f"dslash_kernel<{args.precision}, 6, *> (all sweeps of one solve)",
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                         else "fallback 6.65 TB/s", "launches_timed": nl.value,
+                         "bytes_per_launch": bytes_per_launch, "avg_launch_us": avg_s * 1e6},
+            "cpu_baseline": cpu_baseline,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "mixed": {"iterations": it_m, "reliable_updates": [r["reliable_updates"] for r in reps],
+                      "true_resid_rel": max(r["true_resid_rel"] for r in reps),
+                      "rel_err_vs_fp64_solution": err_vs_fp64},
+            "fp64": {"solves_per_s": 1.0 / fp64_s, "iterations": rep64["iterations"],
+                     "true_resid_rel": rep64["true_resid_rel"], "seconds": fp64_s},
+            "speedup_mixed_vs_fp64": value / ws * fp64_s,
+            "dslash_gbs": dg,
+        }
+        print(json.dumps(line))
+    system.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -56,6 +56,9 @@ SIGNATURES = {
     "c2q_last_error": (C.c_char_p, [_P]),
     "c2q_ctx_synchronize": (C.c_int, [_P]),
     "c2q_ctx_launch_count": (C.c_longlong, [_P]),
+    "c2q_ctx_profile": (C.c_int, [_P, C.c_int]),
+    "c2q_ctx_profile_read": (C.c_int, [_P, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]),
     "c2q_gauge_create": (C.c_int, [_P, C.POINTER(CLattice), C.POINTER(_P)]),
     "c2q_gauge_upload": (C.c_int, [_P, _D]),
     "c2q_gauge_download": (C.c_int, [_P, _D]),

@@ -41,6 +41,16 @@ struct c2q_ctx {
     void* staging          = nullptr;
     size_t staging_cap     = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // optional per-launch dslash timing (c2q_ctx_profile)
+    bool profiling = false;
+    struct Timed {
+        cudaEvent_t a, b;
+        int prec;
+        double sites;
+        double bytes;  // algorithmic bytes of the launch
+    };
+    std::vector<Timed> timed;
+    std::vector<cudaEvent_t> event_pool;
 };
 
 struct c2q_gauge {

@@ -320,10 +320,38 @@ static int dslash_typed(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_
     }
     prm.red = red_args(ctx, dot.fin);
     const bool r12 = gkind == G64R12 || gkind == G32R12 || gkind == G16R12;
+    c2q_ctx::Timed tm{};
+    if (ctx->profiling) {
+        auto get = [&]() {
+            cudaEvent_t e;
+            if (!ctx->event_pool.empty()) {
+                e = ctx->event_pool.back();
+                ctx->event_pool.pop_back();
+            } else {
+                cudaEventCreate(&e);
+            }
+            return e;
+        };
+        tm.a     = get();
+        tm.b     = get();
+        tm.prec  = P;
+        tm.sites = (double)out->geom.seo;
+        // compulsory traffic per output site: 8 links (each read once per sweep),
+        // the input spinor (each read once through L2 reuse), the output, plus
+        // the epilogue/reduction operands read at the output site
+        const double sp = P == 64 ? 192.0 : (P == 32 ? 96.0 : 52.0);
+        const double lk = (r12 ? 12.0 : 18.0) * (P == 64 ? 8.0 : (P == 32 ? 4.0 : 2.0));
+        tm.bytes = tm.sites * (8.0 * lk + sp * (2.0 + (epi == EPI_AXPY ? 1.0 : 0.0) + (dot.mode == DOT_Y ? 1.0 : 0.0)));
+        cudaEventRecord(tm.a, ctx->stream);
+    }
     if (r12)
         dslash_dispatch<P, 6>(prm, epi, dot.mode, blocks, ctx->stream);
     else
         dslash_dispatch<P, 9>(prm, epi, dot.mode, blocks, ctx->stream);
+    if (ctx->profiling) {
+        cudaEventRecord(tm.b, ctx->stream);
+        ctx->timed.push_back(tm);
+    }
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
@@ -537,6 +565,8 @@ using namespace c2q;
 // ==================================================================== C ABI
 extern "C" {
 
+static void profile_recycle(c2q_ctx* ctx);
+
 C2Q_EXPORT const char* c2q_version(void) { return "cl2qcd-b200 0.1 (sm_100a)"; }
 
 C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream)
@@ -596,6 +626,8 @@ C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx)
     cudaFree(ctx->scalars);
     cudaFree(ctx->staging);
     if (ctx->host_pinned) cudaFreeHost(ctx->host_pinned);
+    profile_recycle(ctx);
+    for (auto e : ctx->event_pool) cudaEventDestroy(e);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -613,6 +645,42 @@ C2Q_EXPORT int c2q_ctx_synchronize(c2q_ctx* ctx)
 }
 
 C2Q_EXPORT long long c2q_ctx_launch_count(const c2q_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+static void profile_recycle(c2q_ctx* ctx)
+{
+    for (auto& t : ctx->timed) {
+        ctx->event_pool.push_back(t.a);
+        ctx->event_pool.push_back(t.b);
+    }
+    ctx->timed.clear();
+}
+
+C2Q_EXPORT int c2q_ctx_profile(c2q_ctx* ctx, int enable)
+{
+    if (!ctx) return C2Q_BAD_ARG;
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    profile_recycle(ctx);
+    ctx->profiling = enable != 0;
+    return C2Q_OK;
+}
+
+C2Q_EXPORT int c2q_ctx_profile_read(c2q_ctx* ctx, int prec, long long* launches, double* total_ms, double* bytes)
+{
+    if (!ctx || !launches || !total_ms || !bytes) return C2Q_BAD_ARG;
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *launches = 0;
+    *total_ms = 0.0;
+    *bytes    = 0.0;
+    for (auto& t : ctx->timed) {
+        if (t.prec != prec) continue;
+        float ms = 0.f;
+        C2Q_CUDA(ctx, cudaEventElapsedTime(&ms, t.a, t.b));
+        *launches += 1;
+        *total_ms += ms;
+        *bytes += t.bytes;
+    }
+    return C2Q_OK;
+}
 
 // ---------------------------------------------------------------- gauge
 C2Q_EXPORT int c2q_gauge_create(c2q_ctx* ctx, const c2q_lattice* lat, c2q_gauge** out)

@@ -143,6 +143,17 @@ C2Q_EXPORT const char* c2q_last_error(const c2q_ctx* ctx);
 C2Q_EXPORT int c2q_ctx_synchronize(c2q_ctx* ctx);
 /* Kernels this library launched on the context since creation (all of them are this library's own). */
 C2Q_EXPORT long long c2q_ctx_launch_count(const c2q_ctx* ctx);
+/* Per-launch timing of the dslash sweeps with CUDA events on the context's
+ * stream (off by default; replaces the reference's enableProfiling,
+ * hardware/device.cpp:181-241).  c2q_ctx_profile(ctx, 1) clears and starts;
+ * c2q_ctx_profile_read synchronises and returns, for sweeps of storage
+ * precision `prec` (64, 32, 16), the number of timed launches, their summed
+ * device time in milliseconds and their summed algorithmic bytes (per output
+ * site: 8 links, the input and output spinors, and the spinors an epilogue or
+ * a fused reduction reads at the output site). */
+C2Q_EXPORT int c2q_ctx_profile(c2q_ctx* ctx, int enable);
+C2Q_EXPORT int c2q_ctx_profile_read(c2q_ctx* ctx, int prec, long long* launches, double* total_ms,
+                                    double* bytes);
 
 /* ---------------- gauge field ---------------- */
 /* Gaugefield device layout + import (physics/lattices/gaugefield.hpp:44-139;
