@@ -38,7 +38,7 @@ REL_TOL = 1e-10
 # FP64 CG iterations this workload needs to reach 1e-10 (the reference's CG is the
 # same algorithm in FP64); used to scale the CPU reference's per-iteration sample
 # to solves/s when the GPU arm is not run in the same process.
-FP64_CG_ITERATIONS = None
+FP64_CG_ITERATIONS = 90  # measured on B200 by this bench (fp64.iterations)
 WORKLOAD = (f"32^3x64 tm-Wilson eo CG on QplusQminus_eo, 1 gaussian source, kappa {KAPPA}, mu {MU}, "
             f"eps {EPS}, antiperiodic T, x0 = 0, true residual {REL_TOL}")
 
@@ -46,8 +46,8 @@ WORKLOAD = (f"32^3x64 tm-Wilson eo CG on QplusQminus_eo, 1 gaussian source, kapp
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=16, choices=[16, 32, 64])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -105,6 +105,14 @@ class ClockSampler:
                                       stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+            return
+        # wait until the sampler produces rows, so the timed region is covered
+        t0 = time.time()
+        while time.time() - t0 < 5.0:
+            self.f.flush()
+            if os.path.getsize(self.f.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.p is None:
@@ -124,7 +132,13 @@ class ClockSampler:
         os.unlink(self.f.name)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
@@ -132,7 +146,7 @@ class ClockSampler:
                 if v.lower().startswith("active"):
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "sm_max_mhz": num(rows[0][2]),
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
@@ -347,6 +361,18 @@ def main():
 
     dg = dslash_gbs()
 
+    # ---- FP32-inner variant of the mixed solver, same problem (reported beside)
+    P32 = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=32, use_rec12=True)
+    solve(P32)
+    rep32 = {}
+    e0.record()
+    nrep = 5
+    for _ in range(nrep):
+        solve(P32, rep32)
+    e1.record()
+    torch.cuda.synchronize()
+    fp32_s = e0.elapsed_time(e1) / 1e3 / nrep
+
     cpu_baseline = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -384,6 +410,8 @@ def main():
                       "rel_err_vs_fp64_solution": err_vs_fp64},
             "fp64": {"solves_per_s": 1.0 / fp64_s, "iterations": rep64["iterations"],
                      "true_resid_rel": rep64["true_resid_rel"], "seconds": fp64_s},
+            "fp32_inner": {"solves_per_s": 1.0 / fp32_s, "iterations": rep32["iterations"],
+                           "reliable_updates": rep32["reliable_updates"], "true_resid_rel": rep32["true_resid_rel"]},
             "speedup_mixed_vs_fp64": value / ws * fp64_s,
             "dslash_gbs": dg,
         }

@@ -71,11 +71,16 @@ struct Geom {
     int vs_h;       // NS^3/2
 };
 
-// Hop coefficient table for one dslash launch: coef[mu][0] forward,
-// coef[mu][1] backward, already multiplied by -kappa (the kernel's overall sign)
-// and, on T links, by the chemical-potential factors.
+// Hop coefficients of one dslash launch.  Each hop is weighted by a phase
+// (boundary phase e^{+/- i theta pi / N}, times the chemical-potential factor
+// on T links): phase[mu][0] forward, phase[mu][1] backward.  The common factor
+// -kappa (the kernel's overall sign; times the link dequantisation scale for
+// FP16 links) is applied once per site, in the epilogue.  Bit 2*mu+dir of
+// real_mask is set when that phase is real.
 struct HopCoef {
     double re[4][2], im[4][2];
+    double scale;
+    unsigned real_mask;
 };
 
 // Epilogue applied to the hopping sum h at each output site.
@@ -164,25 +169,51 @@ struct SpinorIO<32> {
     }
 };
 
-// FP16 fixed point: value = q / 32767 * norm, norm = max |real component|.
+// FP16 fixed point (16-bit integers with a per-site scale): a real component
+// v of a site whose largest |component| is `norm` is stored as the biased
+// 16-bit word u = q + 32768, q = rint(v * 32767 / norm) in [-32767, 32767].
+// Decoding is exact and avoids the int->float conversion unit: one byte
+// permute builds the float 2^23 + u, one add subtracts 2^23 + 32768 (= q).
+__device__ __forceinline__ float dq_lo(unsigned w)
+{
+    return __int_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8421376.0f;
+}
+__device__ __forceinline__ float dq_hi(unsigned w)
+{
+    return __int_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8421376.0f;
+}
+__device__ __forceinline__ unsigned eq_pair(float re, float im, float inv)
+{
+    const int lo = __float2int_rn(re * inv) + 32768;
+    const int hi = __float2int_rn(im * inv) + 32768;
+    return (unsigned)(lo & 0xffff) | ((unsigned)hi << 16);
+}
+
 template <>
 struct SpinorIO<16> {
     using R = float;
-    static __device__ __forceinline__ void load(const SpinorPtr<16>& f, int stride, int i, Cplx<R> s[12])
+    // raw words (complex k in word k: re low half, im high half) and the scale norm/32767
+    static __device__ __forceinline__ void load_raw(const SpinorPtr<16>& f, int stride, int i, unsigned w[12],
+                                                    float* sc)
     {
-        const int4* p    = static_cast<const int4*>(f.data);
-        const float sc   = __ldg(f.norm + i) * (1.0f / 32767.0f);
+        const uint4* p = static_cast<const uint4*>(f.data);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            int4 v                = __ldg(p + (size_t)k * stride + i);
-            const int w[4]        = {v.x, v.y, v.z, v.w};
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const short lo = (short)(w[j] & 0xffff);
-                const short hi = (short)(((unsigned)w[j]) >> 16);
-                s[4 * k + j]   = {sc * (float)lo, sc * (float)hi};
-            }
+            const uint4 v = __ldg(p + (size_t)k * stride + i);
+            w[4 * k]      = v.x;
+            w[4 * k + 1]  = v.y;
+            w[4 * k + 2]  = v.z;
+            w[4 * k + 3]  = v.w;
         }
+        *sc = __ldg(f.norm + i) * (1.0f / 32767.0f);
+    }
+    static __device__ __forceinline__ void load(const SpinorPtr<16>& f, int stride, int i, Cplx<R> s[12])
+    {
+        unsigned w[12];
+        float sc;
+        load_raw(f, stride, i, w, &sc);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) s[k] = {sc * dq_lo(w[k]), sc * dq_hi(w[k])};
     }
     static __device__ __forceinline__ void store(const SpinorPtr<16>& f, int stride, int i, const Cplx<R> s[12])
     {
@@ -190,18 +221,13 @@ struct SpinorIO<16> {
 #pragma unroll
         for (int k = 0; k < 12; ++k) mx = fmaxf(mx, fmaxf(fabsf(s[k].re), fabsf(s[k].im)));
         const float inv = mx > 0.f ? 32767.0f / mx : 0.f;
-        int4* p         = static_cast<int4*>(f.data);
+        uint4* p        = static_cast<uint4*>(f.data);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            int w[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int lo = __float2int_rn(s[4 * k + j].re * inv);
-                const int hi = __float2int_rn(s[4 * k + j].im * inv);
-                w[j]         = (lo & 0xffff) | (hi << 16);
-            }
-            p[(size_t)k * stride + i] = make_int4(w[0], w[1], w[2], w[3]);
-        }
+        for (int k = 0; k < 3; ++k)
+            p[(size_t)k * stride + i] = make_uint4(eq_pair(s[4 * k].re, s[4 * k].im, inv),
+                                                   eq_pair(s[4 * k + 1].re, s[4 * k + 1].im, inv),
+                                                   eq_pair(s[4 * k + 2].re, s[4 * k + 2].im, inv),
+                                                   eq_pair(s[4 * k + 3].re, s[4 * k + 3].im, inv));
         f.norm[i] = mx;
     }
 };
@@ -240,34 +266,39 @@ struct LinkIO<32, NL> {
     }
 };
 
-// FP16 links: entries of an SU(3) matrix are bounded by 1 in magnitude, so a
-// fixed scale of 1/32767 is used (no per-link norm).
+// FP16 links: 12-real only.  Entries of an SU(3) matrix are bounded by 1, so
+// a fixed scale is used: u = q + 32768, q = rint(v * 32767) (same biased
+// encoding as the spinors).  Rows 0 and 1 are three uint2 lanes (complex 2j,
+// 2j+1 in lane j).  load_q returns the entries in units of 1/32767.
 template <int NL>
 struct LinkIO<16, NL> {
+    static_assert(NL == 6, "FP16 links are stored 12-real");
     using R = float;
-    static __device__ __forceinline__ void load(const void* base, size_t lane_stride, size_t idx, Cplx<R> u[9])
+    static __device__ __forceinline__ void load_q(const void* base, size_t lane_stride, size_t idx, Cplx<R> u[9])
     {
-        const short2* p = static_cast<const short2*>(base);
-        const float sc  = 1.0f / 32767.0f;
+        const uint2* p = static_cast<const uint2*>(base);
 #pragma unroll
-        for (int k = 0; k < NL; ++k) {
-            short2 v = __ldg(p + k * lane_stride + idx);
-            u[k]     = {sc * (float)v.x, sc * (float)v.y};
+        for (int j = 0; j < 3; ++j) {
+            const uint2 v = __ldg(p + j * lane_stride + idx);
+            u[2 * j]      = {dq_lo(v.x), dq_hi(v.x)};
+            u[2 * j + 1]  = {dq_lo(v.y), dq_hi(v.y)};
         }
     }
 };
 
 // Rebuild row 2 of an SU(3) matrix from rows 0 and 1: row2 = conj(row0 x row1).
+// With rows held in units of a scale s (U = s Q), row 2 in the same units is
+// s * conj(q0 x q1): pass `s` for quantised links, 1 otherwise.
 template <typename R>
-__device__ __forceinline__ void reconstruct_row2(Cplx<R> u[9])
+__device__ __forceinline__ void reconstruct_row2(Cplx<R> u[9], R s = R(1))
 {
     // (a x b)_0 = a1 b2 - a2 b1, etc.
     Cplx<R> c0 = cmul(u[1], u[5]) - cmul(u[2], u[4]);
     Cplx<R> c1 = cmul(u[2], u[3]) - cmul(u[0], u[5]);
     Cplx<R> c2 = cmul(u[0], u[4]) - cmul(u[1], u[3]);
-    u[6]       = {c0.re, -c0.im};
-    u[7]       = {c1.re, -c1.im};
-    u[8]       = {c2.re, -c2.im};
+    u[6]       = {s * c0.re, -s * c0.im};
+    u[7]       = {s * c1.re, -s * c1.im};
+    u[8]       = {s * c2.re, -s * c2.im};
 }
 
 }  // namespace c2q

@@ -82,12 +82,10 @@ struct Proj<3> {  // Z
 };
 
 // One half-spinor channel: acc_a += k U h, acc_p += conj(c) k U h, h = psi_a + c psi_p.
-template <typename R, int A, int PP, int CK, bool DAG>
-__device__ __forceinline__ void hop_channel(Cplx<R> acc[12], const Cplx<R> psi[12], const Cplx<R> u[9], Cplx<R> k)
+// KREAL: k is real (k.im ignored).
+template <typename R, int A, int PP, int CK, bool DAG, bool KREAL>
+__device__ __forceinline__ void hop_channel(Cplx<R> acc[12], const Cplx<R> h[3], const Cplx<R> u[9], Cplx<R> k)
 {
-    Cplx<R> h[3];
-#pragma unroll
-    for (int col = 0; col < 3; ++col) h[col] = psi[3 * A + col] + mul_unit<CK>(psi[3 * PP + col]);
 #pragma unroll
     for (int r = 0; r < 3; ++r) {
         Cplx<R> s;
@@ -100,51 +98,110 @@ __device__ __forceinline__ void hop_channel(Cplx<R> acc[12], const Cplx<R> psi[1
             s = s + cmulc(u[1 * 3 + r], h[1]);
             s = s + cmulc(u[2 * 3 + r], h[2]);
         }
-        const Cplx<R> w = cmul(s, k);
+        const Cplx<R> w = KREAL ? cmk<R>(s.re * k.re, s.im * k.re) : cmul(s, k);
         acc[3 * A + r]  = acc[3 * A + r] + w;
         acc[3 * PP + r] = acc[3 * PP + r] + mul_unit<ConjUnit<CK>::value>(w);
     }
 }
 
-template <typename R, int MU, bool BACK>
-__device__ __forceinline__ void hop(Cplx<R> acc[12], const Cplx<R> psi[12], const Cplx<R> u[9], Cplx<R> k)
+// Projected half spinors of a (decoded) spinor for channel A with partner PP and unit CK.
+template <typename R, int A, int PP, int CK>
+__device__ __forceinline__ void project(Cplx<R> h[3], const Cplx<R> psi[12])
 {
-    using T         = Proj<MU>;
+#pragma unroll
+    for (int col = 0; col < 3; ++col) h[col] = psi[3 * A + col] + mul_unit<CK>(psi[3 * PP + col]);
+}
+// Same from FP16 raw words (values in units of the site's scale).
+template <int A, int PP, int CK>
+__device__ __forceinline__ void project_raw(Cplx<float> h[3], const unsigned w[12])
+{
+#pragma unroll
+    for (int col = 0; col < 3; ++col) {
+        const Cplx<float> a = {dq_lo(w[3 * A + col]), dq_hi(w[3 * A + col])};
+        const Cplx<float> b = {dq_lo(w[3 * PP + col]), dq_hi(w[3 * PP + col])};
+        h[col]              = a + mul_unit<CK>(b);
+    }
+}
+
+template <typename R, int MU, bool BACK, bool KREAL>
+__device__ __forceinline__ void hop_decoded(Cplx<R> acc[12], const Cplx<R> psi[12], const Cplx<R> u[9], Cplx<R> k)
+{
+    using T          = Proj<MU>;
     constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
     constexpr int c1 = BACK ? NegUnit<T::c1>::value : T::c1;
-    hop_channel<R, 0, T::p0, c0, BACK>(acc, psi, u, k);
-    hop_channel<R, 1, T::p1, c1, BACK>(acc, psi, u, k);
+    Cplx<R> h[3];
+    project<R, 0, T::p0, c0>(h, psi);
+    hop_channel<R, 0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
+    project<R, 1, T::p1, c1>(h, psi);
+    hop_channel<R, 1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
+}
+
+template <int MU, bool BACK, bool KREAL>
+__device__ __forceinline__ void hop_raw(Cplx<float> acc[12], const unsigned w[12], const Cplx<float> u[9],
+                                        Cplx<float> k)
+{
+    using T          = Proj<MU>;
+    constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
+    constexpr int c1 = BACK ? NegUnit<T::c1>::value : T::c1;
+    Cplx<float> h[3];
+    project_raw<0, T::p0, c0>(h, w);
+    hop_channel<float, 0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
+    project_raw<1, T::p1, c1>(h, w);
+    hop_channel<float, 1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
+}
+
+// One hop: load the neighbour spinor and the link, weight by the hop phase.
+template <int P, int NL, int MU, bool BACK>
+__device__ __forceinline__ void do_hop(Cplx<typename Prec<P>::R> acc[12], const DslashParams<P>& prm,
+                                       const char* links, size_t link_idx, int i_nb)
+{
+    using R          = typename Prec<P>::R;
+    const Geom& g    = prm.g;
+    const size_t ls  = (size_t)g.stride;
+    const int d      = BACK ? 1 : 0;
+    const bool kreal = (prm.c.real_mask >> (2 * MU + d)) & 1u;
+    Cplx<R> u[9];
+    if constexpr (P == 16) {
+        unsigned w[12];
+        float sc;
+        SpinorIO<16>::load_raw(prm.in, g.stride, i_nb, w, &sc);
+        LinkIO<16, NL>::load_q(links, ls, link_idx, u);
+        reconstruct_row2(u, 1.0f / 32767.0f);
+        const Cplx<float> k = {(float)prm.c.re[MU][d] * sc, (float)prm.c.im[MU][d] * sc};
+        if (kreal)
+            hop_raw<MU, BACK, true>(acc, w, u, k);
+        else
+            hop_raw<MU, BACK, false>(acc, w, u, k);
+    } else {
+        Cplx<R> psi[12];
+        SpinorIO<P>::load(prm.in, g.stride, i_nb, psi);
+        LinkIO<P, NL>::load(links, ls, link_idx, u);
+        if (NL == 6) reconstruct_row2(u);
+        const Cplx<R> k = cmk<R>((R)prm.c.re[MU][d], (R)prm.c.im[MU][d]);
+        if (kreal)
+            hop_decoded<R, MU, BACK, true>(acc, psi, u, k);
+        else
+            hop_decoded<R, MU, BACK, false>(acc, psi, u, k);
+    }
 }
 
 template <int P, int NL, int MU>
 __device__ __forceinline__ void do_direction(Cplx<typename Prec<P>::R> acc[12], const DslashParams<P>& prm,
                                              int i_fwd, int i_bwd, int i_site)
 {
-    using R                 = typename Prec<P>::R;
-    const Geom& g           = prm.g;
-    const size_t ls         = (size_t)g.stride;
-    const int po            = prm.out_parity;
+    const size_t ls       = (size_t)prm.g.stride;
+    const int po          = prm.out_parity;
     // element size of one complex lane entry in this precision
-    constexpr size_t esz    = P == 64 ? 16 : (P == 32 ? 8 : 4);
-    const char* gbase       = static_cast<const char*>(prm.gauge);
-    const char* fwd_links   = gbase + (size_t)((po * 4 + MU) * NL) * ls * esz;
-    const char* bwd_links   = gbase + (size_t)(((1 - po) * 4 + MU) * NL) * ls * esz;
-
-    Cplx<R> psi[12], u[9];
-    // forward: U_mu(x) psi(x+mu)
-    SpinorIO<P>::load(prm.in, g.stride, i_fwd, psi);
-    LinkIO<P, NL>::load(fwd_links, ls, (size_t)i_site, u);
-    if (NL == 6) reconstruct_row2(u);
-    hop<R, MU, false>(acc, psi, u, cmk<R>((R)prm.c.re[MU][0], (R)prm.c.im[MU][0]));
-    // backward: U_mu(x-mu)^dagger psi(x-mu)
-    SpinorIO<P>::load(prm.in, g.stride, i_bwd, psi);
-    LinkIO<P, NL>::load(bwd_links, ls, (size_t)i_bwd, u);
-    if (NL == 6) reconstruct_row2(u);
-    hop<R, MU, true>(acc, psi, u, cmk<R>((R)prm.c.re[MU][1], (R)prm.c.im[MU][1]));
+    constexpr size_t esz  = P == 64 ? 16 : (P == 32 ? 8 : 4);
+    const char* gbase     = static_cast<const char*>(prm.gauge);
+    const char* fwd_links = gbase + (size_t)((po * 4 + MU) * NL) * ls * esz;
+    const char* bwd_links = gbase + (size_t)(((1 - po) * 4 + MU) * NL) * ls * esz;
+    do_hop<P, NL, MU, false>(acc, prm, fwd_links, (size_t)i_site, i_fwd);  // U_mu(x) psi(x+mu)
+    do_hop<P, NL, MU, true>(acc, prm, bwd_links, (size_t)i_bwd, i_bwd);    // U_mu(x-mu)^dagger psi(x-mu)
 }
 
 template <int P, int NL, int EPI, int DOT>
-__global__ void __launch_bounds__(128) dslash_kernel(const DslashParams<P> prm)
+__global__ void __launch_bounds__(128, P == 16 ? 7 : 1) dslash_kernel(const DslashParams<P> prm)
 {
     using R       = typename Prec<P>::R;
     const Geom& g = prm.g;
@@ -186,8 +243,14 @@ __global__ void __launch_bounds__(128) dslash_kernel(const DslashParams<P> prm)
                                    xh + g.nsh * (y + g.ns * (zm + g.ns * t)), i);
         }
 
-        if (EPI == EPI_DIAG) {
-            const Cplx<R> f1 = cmk<R>((R)prm.e.f1re, (R)prm.e.f1im), f2 = cmk<R>((R)prm.e.f2re, (R)prm.e.f2im);
+        // the hopping sum is h = scale * acc (scale = -kappa, times the link dequantisation scale)
+        const R sc = (R)prm.c.scale;
+        if (EPI == EPI_PLAIN) {
+#pragma unroll
+            for (int k = 0; k < 12; ++k) acc[k] = cmk<R>(sc * acc[k].re, sc * acc[k].im);
+        } else if (EPI == EPI_DIAG) {
+            const Cplx<R> f1 = cmk<R>((R)prm.e.f1re * sc, (R)prm.e.f1im * sc);
+            const Cplx<R> f2 = cmk<R>((R)prm.e.f2re * sc, (R)prm.e.f2im * sc);
 #pragma unroll
             for (int k = 0; k < 12; ++k) acc[k] = cmul(k < 6 ? f1 : f2, acc[k]);
         } else if (EPI == EPI_AXPY) {
@@ -196,7 +259,8 @@ __global__ void __launch_bounds__(128) dslash_kernel(const DslashParams<P> prm)
             const Cplx<R> f1 = cmk<R>((R)prm.e.f1re, (R)prm.e.f1im), f2 = cmk<R>((R)prm.e.f2re, (R)prm.e.f2im);
 #pragma unroll
             for (int k = 0; k < 12; ++k) {
-                Cplx<R> r = cmul(k < 6 ? f1 : f2, xv[k]) - acc[k];
+                const Cplx<R> m = cmul(k < 6 ? f1 : f2, xv[k]);
+                Cplx<R> r       = cmk<R>(m.re - sc * acc[k].re, m.im - sc * acc[k].im);
                 if (prm.e.gamma5 && k >= 6) r = cmk<R>(-r.re, -r.im);
                 acc[k] = r;
             }

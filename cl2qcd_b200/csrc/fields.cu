@@ -60,8 +60,8 @@ HopCoef hop_coef(const c2q_lattice& lat, double kappa)
     for (int mu = 0; mu < 4; ++mu) {
         const double ang = mu == 0 ? (lat.theta_t * PI_REF) / (double)lat.nt : (lat.theta_s * PI_REF) / (double)lat.ns;
         const double re = as_build_option(std::cos(ang)), im = as_build_option(std::sin(ang));
-        double fre = kappa * re, fim = kappa * im;   // forward  kappa e^{+i phi}
-        double bre = kappa * re, bim = -kappa * im;  // backward kappa e^{-i phi}
+        double fre = re, fim = im;   // forward  e^{+i phi}
+        double bre = re, bim = -im;  // backward e^{-i phi}
         if (mu == 0 && (lat.use_cp_re || lat.use_cp_im)) {
             // chemical potential on T links (ocl_kernel/fermionmatrix_eo.cl:115-121, 222-228):
             // forward U e^{cp_re} e^{i cp_im}, backward (U e^{-cp_re} e^{i cp_im})^dagger
@@ -78,11 +78,17 @@ HopCoef hop_coef(const c2q_lattice& lat, double kappa)
             bre = r;
             bim = i;
         }
-        c.re[mu][0] = -fre;
-        c.im[mu][0] = -fim;
-        c.re[mu][1] = -bre;
-        c.im[mu][1] = -bim;
+        // the phases carry no kappa: -kappa is applied once per site (HopCoef::scale)
+        c.re[mu][0] = fre;
+        c.im[mu][0] = fim;
+        c.re[mu][1] = bre;
+        c.im[mu][1] = bim;
     }
+    c.scale     = -kappa;
+    c.real_mask = 0;
+    for (int mu = 0; mu < 4; ++mu)
+        for (int d = 0; d < 2; ++d)
+            if (c.im[mu][d] == 0.0) c.real_mask |= 1u << (2 * mu + d);
     return c;
 }
 
@@ -236,11 +242,30 @@ __global__ void gauge_convert_kernel(const double2* __restrict__ in, T* __restri
             dst[(size_t)k * g.stride] = v;
         } else if constexpr (sizeof(T) == 8) {
             dst[(size_t)k * g.stride] = T{(float)v.x, (float)v.y};
-        } else {
-            const double cx = fmin(1.0, fmax(-1.0, v.x)), cy = fmin(1.0, fmax(-1.0, v.y));
-            dst[(size_t)k * g.stride] = T{(short)__double2int_rn(cx * 32767.0), (short)__double2int_rn(cy * 32767.0)};
         }
     }
+}
+
+// FP64 9-lane store -> FP16 12-real: rows 0 and 1 as three uint2 lanes of
+// biased 16-bit fixed point (u = rint(v * 32767) + 32768, v clamped to [-1, 1]).
+__device__ __forceinline__ unsigned enc16(double2 v)
+{
+    const double cx = fmin(1.0, fmax(-1.0, v.x)), cy = fmin(1.0, fmax(-1.0, v.y));
+    const int lo    = __double2int_rn(cx * 32767.0) + 32768;
+    const int hi    = __double2int_rn(cy * 32767.0) + 32768;
+    return (unsigned)(lo & 0xffff) | ((unsigned)hi << 16);
+}
+__global__ void gauge_convert16_kernel(const double2* __restrict__ in, uint2* __restrict__ out, Geom g)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 8LL * g.stride) return;
+    const int blk = (int)(t / g.stride), i = (int)(t - (long long)blk * g.stride);
+    const double2* src = in + (size_t)blk * 9 * g.stride + i;
+    uint2* dst         = out + (size_t)blk * 3 * g.stride + i;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        dst[(size_t)j * g.stride] = make_uint2(enc16(src[(size_t)(2 * j) * g.stride]),
+                                               enc16(src[(size_t)(2 * j + 1) * g.stride]));
 }
 
 int gauge_ensure(c2q_gauge* g, int kind)
@@ -266,7 +291,7 @@ int gauge_ensure(c2q_gauge* g, int kind)
         case G64R12: gauge_convert_kernel<double2, 6><<<blocks, threads, 0, ctx->stream>>>(src, (double2*)p, g->geom); break;
         case G32: gauge_convert_kernel<float2, 9><<<blocks, threads, 0, ctx->stream>>>(src, (float2*)p, g->geom); break;
         case G32R12: gauge_convert_kernel<float2, 6><<<blocks, threads, 0, ctx->stream>>>(src, (float2*)p, g->geom); break;
-        case G16R12: gauge_convert_kernel<short2, 6><<<blocks, threads, 0, ctx->stream>>>(src, (short2*)p, g->geom); break;
+        case G16R12: gauge_convert16_kernel<<<blocks, threads, 0, ctx->stream>>>(src, (uint2*)p, g->geom); break;
     }
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
@@ -311,6 +336,7 @@ static int dslash_typed(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_
     prm.gauge      = g->store[gkind].data;
     prm.g          = out->geom;
     prm.c          = hop_coef(out->lat, kappa);
+    if (P == 16) prm.c.scale *= 1.0 / 32767.0;  // FP16 links are applied in units of 1/32767
     prm.e          = e;
     prm.out_parity = out_parity;
     const int blocks = (out->geom.seo + 127) / 128;
@@ -344,10 +370,14 @@ static int dslash_typed(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_
         tm.bytes = tm.sites * (8.0 * lk + sp * (2.0 + (epi == EPI_AXPY ? 1.0 : 0.0) + (dot.mode == DOT_Y ? 1.0 : 0.0)));
         cudaEventRecord(tm.a, ctx->stream);
     }
-    if (r12)
-        dslash_dispatch<P, 6>(prm, epi, dot.mode, blocks, ctx->stream);
-    else
-        dslash_dispatch<P, 9>(prm, epi, dot.mode, blocks, ctx->stream);
+    if constexpr (P == 16) {
+        dslash_dispatch<16, 6>(prm, epi, dot.mode, blocks, ctx->stream);
+    } else {
+        if (r12)
+            dslash_dispatch<P, 6>(prm, epi, dot.mode, blocks, ctx->stream);
+        else
+            dslash_dispatch<P, 9>(prm, epi, dot.mode, blocks, ctx->stream);
+    }
     if (ctx->profiling) {
         cudaEventRecord(tm.b, ctx->stream);
         ctx->timed.push_back(tm);

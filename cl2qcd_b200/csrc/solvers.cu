@@ -135,6 +135,15 @@ int true_residual(c2q_ctx* ctx, int op, const c2q_gauge* g, const c2q_spinor_eo*
     return saxpy_norm(ctx, r, Cx{1, 0}, r, b, FIN_STORE_RESULT, r2);
 }
 
+// |x|^2 (to skip A x when the start vector is zero)
+int norm2(c2q_ctx* ctx, const c2q_spinor_eo* x, double* out)
+{
+    Cx c;
+    int rc = dot_read(ctx, x, x, &c);
+    *out   = c.re;
+    return rc;
+}
+
 bool validate(c2q_ctx* ctx, const c2q_spinor_eo* x, const c2q_gauge* g, const c2q_spinor_eo* b,
               const c2q_solver_params* p, int* rc)
 {
@@ -202,6 +211,7 @@ int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2
     int iter = 0, status = C2Q_DID_NOT_SOLVE;
     double resid = std::numeric_limits<double>::quiet_NaN();
     bool force_refresh = false;
+    double r2_confirmed = -1.0;  // true residual of the returned solution, when already computed
     for (iter = 0; iter < P->cgmax || iter < P->min_iter; iter++) {
         if (iter % P->iter_refresh == 0 || force_refresh) {
             force_refresh = false;
@@ -232,7 +242,8 @@ int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2
                     rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, t2, t1, v, &r2t, &sweeps);
                     if (rc) return rc;
                     if (r2t <= P->rel_tol * P->rel_tol * b2 || (P->prec > 0 && r2t < P->prec)) {
-                        status = iter;
+                        status       = iter;
+                        r2_confirmed = r2t;
                         break;
                     }
                     force_refresh = true;  // iterated residual drifted: restart from the true residual
@@ -245,9 +256,11 @@ int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2
         rc = launch_cg_p(ctx, p, rn);  // p = rn + beta p
         if (rc) return rc;
     }
-    double r2t = 0;
-    rc         = true_residual(ctx, op, g, x, b, kappa, mubar, action, rn, t1, t2, &r2t, &sweeps);
-    if (rc) return rc;
+    double r2t = r2_confirmed;
+    if (r2t < 0) {
+        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, rn, t1, t2, &r2t, &sweeps);
+        if (rc) return rc;
+    }
     finish_report(rep, status, iter, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sweeps);
     if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
     if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "NAN occured in the CG residual");
@@ -333,13 +346,22 @@ int cg_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c
     rc        = saxpy_norm(ctx, r64, Cx{0, 0}, b, b, FIN_STORE_RESULT, &b2);
     if (rc) return rc;
     const double thr = stop_threshold(P, b2);
-    double r2        = 0;
-    rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
+    double r2        = 0, x2 = 0;
+    rc               = norm2(ctx, x, &x2);
+    if (rc) return rc;
+    if (x2 == 0.0) {
+        // r = b - A 0 = b: no operator application needed
+        rc = copy_field(ctx, r64, b);
+        r2 = b2;
+    } else {
+        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
+    }
     if (rc) return rc;
     int iter = 0, status = C2Q_DID_NOT_SOLVE;
-    double resid = r2;
+    double resid = r2, r2_confirmed = -1.0;
     if (r2 < thr) {
-        status = 0;
+        status       = 0;
+        r2_confirmed = r2;
     } else {
         rc = launch_convert(ctx, rs, r64);
         if (!rc) rc = c2q_spinor_eo_zero(xs);
@@ -376,7 +398,8 @@ int cg_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c
                     ++reliable;
                     resid = r2;
                     if (r2 < thr) {
-                        status = iter + 1;
+                        status       = iter + 1;
+                        r2_confirmed = r2;
                         break;
                     }
                     rc = launch_convert(ctx, rs, r64);
@@ -401,9 +424,11 @@ int cg_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c
             if (rc2) return rc2;
         }
     }
-    double r2t = 0;
-    rc         = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2t, &sweeps);
-    if (rc) return rc;
+    double r2t = r2_confirmed;
+    if (r2t < 0) {
+        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2t, &sweeps);
+        if (rc) return rc;
+    }
     finish_report(rep, status, iter, reliable, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sweeps);
     if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
     if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "NAN occured in the mixed-precision CG residual");

@@ -23,6 +23,7 @@ Everything runs in the CUDA library; nothing here computes on the CPU.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -71,6 +72,11 @@ class System:
         if rc != 0:
             raise L.C2QError(rc, "c2q_ctx_create failed (no CUDA device?)")
         self.h = h
+        # device objects of this context; they are destroyed before the context
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, obj):
+        self._children.add(obj)
 
     def synchronize(self):
         _check(self.lib.c2q_ctx_synchronize(self.h), self.h, self.lib)
@@ -81,6 +87,8 @@ class System:
 
     def close(self):
         if getattr(self, "h", None):
+            for child in list(self._children):
+                child._destroy()
             self.lib.c2q_ctx_destroy(self.h)
             self.h = None
 
@@ -135,6 +143,7 @@ class Gaugefield:
         lc = lattice.c()
         _check(lib.c2q_gauge_create(system.h, C.byref(lc), C.byref(h)), system.h, lib)
         self.h = h
+        system._adopt(self)
         if aos is not None:
             self.upload(aos)
 
@@ -152,11 +161,15 @@ class Gaugefield:
     def device_bytes(self):
         return self.system.lib.c2q_gauge_device_bytes(self.h)
 
+    def _destroy(self):
+        # a context outlives its objects: nothing to do once the context is closed
+        if getattr(self, "h", None) and getattr(self.system, "h", None):
+            self.system.lib.c2q_gauge_destroy(self.h)
+        self.h = None
+
     def __del__(self):
         try:
-            if getattr(self, "h", None):
-                self.system.lib.c2q_gauge_destroy(self.h)
-                self.h = None
+            self._destroy()
         except Exception:
             pass
 
@@ -169,6 +182,7 @@ class Spinorfield_eo:
         lc = lattice.c()
         _check(lib.c2q_spinor_eo_create(system.h, C.byref(lc), C.byref(h)), system.h, lib)
         self.h = h
+        system._adopt(self)
         if aos is not None:
             self.load(aos)
 
@@ -192,11 +206,14 @@ class Spinorfield_eo:
     def gamma5(self):
         _check(self.system.lib.c2q_gamma5_eo(self.h), self.system.h, self.system.lib)
 
+    def _destroy(self):
+        if getattr(self, "h", None) and getattr(self.system, "h", None):
+            self.system.lib.c2q_spinor_eo_destroy(self.h)
+        self.h = None
+
     def __del__(self):
         try:
-            if getattr(self, "h", None):
-                self.system.lib.c2q_spinor_eo_destroy(self.h)
-                self.h = None
+            self._destroy()
         except Exception:
             pass
 

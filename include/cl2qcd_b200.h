@@ -138,6 +138,8 @@ typedef struct {
  * if non-NULL, else the context creates its own.  Replaces hardware::System /
  * hardware::Device (hardware/system.cpp:117-200, hardware/device.cpp:79). */
 C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream);
+/* Every gauge and spinor object created on a context must be destroyed before
+ * the context (they use its stream). */
 C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx);
 C2Q_EXPORT const char* c2q_last_error(const c2q_ctx* ctx);
 C2Q_EXPORT int c2q_ctx_synchronize(c2q_ctx* ctx);
