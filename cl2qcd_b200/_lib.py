@@ -86,6 +86,7 @@ SIGNATURES = {
     "c2q_scalar_product": (C.c_int, [_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "c2q_squarenorm": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "c2q_saxpy_AND_squarenorm": (C.c_int, [_P, C.c_double, C.c_double, _P, _P, C.POINTER(C.c_double)]),
+    "c2q_scalar_product_eo_noalloc": (C.c_int, [_P, _P, C.c_int, C.c_int, _P, _P]),
     "c2q_solver_params_default": (None, [C.POINTER(CSolverParams)]),
     "c2q_cg": (C.c_int, [_P, C.c_int, _P, _P, C.c_double, C.c_double, C.c_int, C.POINTER(CSolverParams),
                          C.POINTER(CSolveReport)]),

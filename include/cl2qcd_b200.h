@@ -216,6 +216,27 @@ C2Q_EXPORT int c2q_squarenorm(const c2q_spinor_eo* x, double* result);
 C2Q_EXPORT int c2q_saxpy_AND_squarenorm(c2q_spinor_eo* out, double alpha_re, double alpha_im,
                                         const c2q_spinor_eo* x, const c2q_spinor_eo* y, double* squarenorm);
 
+/* Scalar product sum conj(x) y of two FP64 eo spinor fields, for callers that
+ * cannot allocate device memory (their memory pool owns the GPU, they cannot
+ * afford the synchronisation an allocation may cause, or their host program
+ * forbids plugins from allocating).  No counterpart in the reference: it is an
+ * addition of this library.
+ *   x_soa, y_soa : caller-owned device buffers in the library's FP64 field
+ *                  layout: 12 complex lanes of double2, component k of site i
+ *                  at element k*stride + i (stride >= n_sites);
+ *   result_dev   : caller-owned device memory for 2 doubles (re, im);
+ *   cuda_stream  : the cudaStream_t to run on (NULL = legacy default stream).
+ * Asynchronous: the result is in result_dev when the stream reaches it.
+ * Allocates nothing: the reduction scratch is a fixed array inside the library
+ * (about 256 KiB per device, held until the process exits); more than
+ * C2Q_NOALLOC_MAX_SITES sites is rejected with C2Q_BAD_ARG (and a message on
+ * stderr).  The first call on a device looks up the scratch's device address,
+ * so make that call before any stream capture.  Calls share the scratch:
+ * calls that overlap on the GPU (other streams or host threads) race. */
+#define C2Q_NOALLOC_MAX_SITES 4194304
+C2Q_EXPORT int c2q_scalar_product_eo_noalloc(const void* x_soa, const void* y_soa, int n_sites, int stride,
+                                             double* result_dev, void* cuda_stream);
+
 /* ---------------- solvers ---------------- */
 C2Q_EXPORT void c2q_solver_params_default(c2q_solver_params* p);
 /* solvers::cg (physics/algorithms/solvers/cg.hpp:41-56, cg.cpp:158-170, 277-400):
