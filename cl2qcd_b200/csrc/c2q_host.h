@@ -41,6 +41,7 @@ struct c2q_ctx {
     void* staging          = nullptr;
     size_t staging_cap     = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ring_ev[4] = {};  // residual ring of the pipelined solvers
     // optional per-launch dslash timing (c2q_ctx_profile)
     bool profiling = false;
     struct Timed {

@@ -60,6 +60,30 @@ __device__ __forceinline__ Cplx<R> cmulc(Cplx<R> a, Cplx<R> b)
     return {a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
 }
 
+// fused multiply-add in the compute type
+__device__ __forceinline__ float fmad(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmad(double a, double b, double c) { return fma(a, b, c); }
+
+// acc += a * b as four FMAs (a sum of complex products written as `s + a*b`
+// would cost a multiply, an FMA and an add per real component)
+template <typename R>
+__device__ __forceinline__ void cmac(Cplx<R>& acc, Cplx<R> a, Cplx<R> b)
+{
+    acc.re = fmad(a.re, b.re, acc.re);
+    acc.re = fmad(-a.im, b.im, acc.re);
+    acc.im = fmad(a.re, b.im, acc.im);
+    acc.im = fmad(a.im, b.re, acc.im);
+}
+// acc += conj(a) * b
+template <typename R>
+__device__ __forceinline__ void cmacc(Cplx<R>& acc, Cplx<R> a, Cplx<R> b)
+{
+    acc.re = fmad(a.re, b.re, acc.re);
+    acc.re = fmad(a.im, b.im, acc.re);
+    acc.im = fmad(a.re, b.im, acc.im);
+    acc.im = fmad(-a.im, b.re, acc.im);
+}
+
 // ------------------------------------------------------------------------
 // lattice geometry and per-launch operator coefficients
 // ------------------------------------------------------------------------
@@ -292,10 +316,14 @@ struct LinkIO<16, NL> {
 template <typename R>
 __device__ __forceinline__ void reconstruct_row2(Cplx<R> u[9], R s = R(1))
 {
-    // (a x b)_0 = a1 b2 - a2 b1, etc.
-    Cplx<R> c0 = cmul(u[1], u[5]) - cmul(u[2], u[4]);
-    Cplx<R> c1 = cmul(u[2], u[3]) - cmul(u[0], u[5]);
-    Cplx<R> c2 = cmul(u[0], u[4]) - cmul(u[1], u[3]);
+    // (a x b)_0 = a1 b2 - a2 b1, etc., as FMA chains
+    const Cplx<R> m2 = {-u[2].re, -u[2].im}, m0 = {-u[0].re, -u[0].im}, m1 = {-u[1].re, -u[1].im};
+    Cplx<R> c0 = cmul(u[1], u[5]);
+    cmac(c0, m2, u[4]);
+    Cplx<R> c1 = cmul(u[2], u[3]);
+    cmac(c1, m0, u[5]);
+    Cplx<R> c2 = cmul(u[0], u[4]);
+    cmac(c2, m1, u[3]);
     u[6]       = {s * c0.re, -s * c0.im};
     u[7]       = {s * c1.re, -s * c1.im};
     u[8]       = {s * c2.re, -s * c2.im};

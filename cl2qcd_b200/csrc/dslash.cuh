@@ -82,7 +82,7 @@ struct Proj<3> {  // Z
 };
 
 // One half-spinor channel: acc_a += k U h, acc_p += conj(c) k U h, h = psi_a + c psi_p.
-// KREAL: k is real (k.im ignored).
+// KREAL: k is real (k.im ignored).  Everything is written as FMA chains.
 template <typename R, int A, int PP, int CK, bool DAG, bool KREAL>
 __device__ __forceinline__ void hop_channel(Cplx<R> acc[12], const Cplx<R> h[3], const Cplx<R> u[9], Cplx<R> k)
 {
@@ -91,16 +91,24 @@ __device__ __forceinline__ void hop_channel(Cplx<R> acc[12], const Cplx<R> h[3],
         Cplx<R> s;
         if (!DAG) {
             s = cmul(u[3 * r + 0], h[0]);
-            s = s + cmul(u[3 * r + 1], h[1]);
-            s = s + cmul(u[3 * r + 2], h[2]);
+            cmac(s, u[3 * r + 1], h[1]);
+            cmac(s, u[3 * r + 2], h[2]);
         } else {
             s = cmulc(u[0 * 3 + r], h[0]);
-            s = s + cmulc(u[1 * 3 + r], h[1]);
-            s = s + cmulc(u[2 * 3 + r], h[2]);
+            cmacc(s, u[1 * 3 + r], h[1]);
+            cmacc(s, u[2 * 3 + r], h[2]);
         }
-        const Cplx<R> w = KREAL ? cmk<R>(s.re * k.re, s.im * k.re) : cmul(s, k);
-        acc[3 * A + r]  = acc[3 * A + r] + w;
-        acc[3 * PP + r] = acc[3 * PP + r] + mul_unit<ConjUnit<CK>::value>(w);
+        // lower row: acc_p += conj(c) * (k s); conj(c) * s is an exact sign/swap
+        const Cplx<R> sp = mul_unit<ConjUnit<CK>::value>(s);
+        if (KREAL) {
+            acc[3 * A + r].re  = fmad(s.re, k.re, acc[3 * A + r].re);
+            acc[3 * A + r].im  = fmad(s.im, k.re, acc[3 * A + r].im);
+            acc[3 * PP + r].re = fmad(sp.re, k.re, acc[3 * PP + r].re);
+            acc[3 * PP + r].im = fmad(sp.im, k.re, acc[3 * PP + r].im);
+        } else {
+            cmac(acc[3 * A + r], s, k);
+            cmac(acc[3 * PP + r], sp, k);
+        }
     }
 }
 
@@ -150,8 +158,13 @@ __device__ __forceinline__ void hop_raw(Cplx<float> acc[12], const unsigned w[12
     hop_channel<float, 1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
 }
 
+// Phase patterns known at compile time (the common boundary conditions): PH_REAL
+// all hop phases real, PH_TCPLX only the T phases complex (antiperiodic time,
+// periodic space), PH_ANY decided per launch from HopCoef::real_mask.
+enum PhasePattern : int { PH_REAL = 0, PH_TCPLX = 1, PH_ANY = 2 };
+
 // One hop: load the neighbour spinor and the link, weight by the hop phase.
-template <int P, int NL, int MU, bool BACK>
+template <int P, int NL, int MU, bool BACK, int PH>
 __device__ __forceinline__ void do_hop(Cplx<typename Prec<P>::R> acc[12], const DslashParams<P>& prm,
                                        const char* links, size_t link_idx, int i_nb)
 {
@@ -159,7 +172,9 @@ __device__ __forceinline__ void do_hop(Cplx<typename Prec<P>::R> acc[12], const 
     const Geom& g    = prm.g;
     const size_t ls  = (size_t)g.stride;
     const int d      = BACK ? 1 : 0;
-    const bool kreal = (prm.c.real_mask >> (2 * MU + d)) & 1u;
+    const bool kreal = PH == PH_REAL ? true
+                       : PH == PH_TCPLX ? (MU != 0)
+                                        : (bool)((prm.c.real_mask >> (2 * MU + d)) & 1u);
     Cplx<R> u[9];
     if constexpr (P == 16) {
         unsigned w[12];
@@ -185,7 +200,7 @@ __device__ __forceinline__ void do_hop(Cplx<typename Prec<P>::R> acc[12], const 
     }
 }
 
-template <int P, int NL, int MU>
+template <int P, int NL, int MU, int PH>
 __device__ __forceinline__ void do_direction(Cplx<typename Prec<P>::R> acc[12], const DslashParams<P>& prm,
                                              int i_fwd, int i_bwd, int i_site)
 {
@@ -196,11 +211,11 @@ __device__ __forceinline__ void do_direction(Cplx<typename Prec<P>::R> acc[12], 
     const char* gbase     = static_cast<const char*>(prm.gauge);
     const char* fwd_links = gbase + (size_t)((po * 4 + MU) * NL) * ls * esz;
     const char* bwd_links = gbase + (size_t)(((1 - po) * 4 + MU) * NL) * ls * esz;
-    do_hop<P, NL, MU, false>(acc, prm, fwd_links, (size_t)i_site, i_fwd);  // U_mu(x) psi(x+mu)
-    do_hop<P, NL, MU, true>(acc, prm, bwd_links, (size_t)i_bwd, i_bwd);    // U_mu(x-mu)^dagger psi(x-mu)
+    do_hop<P, NL, MU, false, PH>(acc, prm, fwd_links, (size_t)i_site, i_fwd);  // U_mu(x) psi(x+mu)
+    do_hop<P, NL, MU, true, PH>(acc, prm, bwd_links, (size_t)i_bwd, i_bwd);    // U_mu(x-mu)^dagger psi(x-mu)
 }
 
-template <int P, int NL, int EPI, int DOT>
+template <int P, int NL, int EPI, int DOT, int PH>
 __global__ void __launch_bounds__(128, P == 16 ? 7 : 1) dslash_kernel(const DslashParams<P> prm)
 {
     using R       = typename Prec<P>::R;
@@ -226,20 +241,20 @@ __global__ void __launch_bounds__(128, P == 16 ? 7 : 1) dslash_kernel(const Dsla
         {  // T
             const int tp = t + 1 == g.nt ? 0 : t + 1, tm = t == 0 ? g.nt - 1 : t - 1;
             const int base = xh + g.nsh * (y + g.ns * z);
-            do_direction<P, NL, 0>(acc, prm, base + g.vs_h * tp, base + g.vs_h * tm, i);
+            do_direction<P, NL, 0, PH>(acc, prm, base + g.vs_h * tp, base + g.vs_h * tm, i);
         }
         {  // X
             const int xp = x + 1 == g.ns ? 0 : x + 1, xm = x == 0 ? g.ns - 1 : x - 1;
-            do_direction<P, NL, 1>(acc, prm, (xp >> 1) + yzt, (xm >> 1) + yzt, i);
+            do_direction<P, NL, 1, PH>(acc, prm, (xp >> 1) + yzt, (xm >> 1) + yzt, i);
         }
         {  // Y
             const int yp = y + 1 == g.ns ? 0 : y + 1, ym = y == 0 ? g.ns - 1 : y - 1;
             const int zt = g.ns * (z + g.ns * t);
-            do_direction<P, NL, 2>(acc, prm, xh + g.nsh * (yp + zt), xh + g.nsh * (ym + zt), i);
+            do_direction<P, NL, 2, PH>(acc, prm, xh + g.nsh * (yp + zt), xh + g.nsh * (ym + zt), i);
         }
         {  // Z
             const int zp = z + 1 == g.ns ? 0 : z + 1, zm = z == 0 ? g.ns - 1 : z - 1;
-            do_direction<P, NL, 3>(acc, prm, xh + g.nsh * (y + g.ns * (zp + g.ns * t)),
+            do_direction<P, NL, 3, PH>(acc, prm, xh + g.nsh * (y + g.ns * (zp + g.ns * t)),
                                    xh + g.nsh * (y + g.ns * (zm + g.ns * t)), i);
         }
 

@@ -301,25 +301,43 @@ int gauge_ensure(c2q_gauge* g, int kind)
 }
 
 // ------------------------------------------------------------------ launches
-template <int P, int NL, int EPI, int DOT>
+template <int P, int NL, int EPI, int DOT, int PH>
 static void dslash_go(const DslashParams<P>& prm, int blocks, cudaStream_t s)
 {
-    dslash_kernel<P, NL, EPI, DOT><<<blocks, 128, 0, s>>>(prm);
+    dslash_kernel<P, NL, EPI, DOT, PH><<<blocks, 128, 0, s>>>(prm);
 }
 
+template <int P, int NL, int PH>
+static void dslash_dispatch_ph(const DslashParams<P>& prm, int epi, int dot, int blocks, cudaStream_t s)
+{
+    switch (epi * 3 + dot) {
+        case 0: dslash_go<P, NL, EPI_PLAIN, DOT_NONE, PH>(prm, blocks, s); break;
+        case 1: dslash_go<P, NL, EPI_PLAIN, DOT_Y, PH>(prm, blocks, s); break;
+        case 2: dslash_go<P, NL, EPI_PLAIN, DOT_SELF, PH>(prm, blocks, s); break;
+        case 3: dslash_go<P, NL, EPI_DIAG, DOT_NONE, PH>(prm, blocks, s); break;
+        case 4: dslash_go<P, NL, EPI_DIAG, DOT_Y, PH>(prm, blocks, s); break;
+        case 5: dslash_go<P, NL, EPI_DIAG, DOT_SELF, PH>(prm, blocks, s); break;
+        case 6: dslash_go<P, NL, EPI_AXPY, DOT_NONE, PH>(prm, blocks, s); break;
+        case 7: dslash_go<P, NL, EPI_AXPY, DOT_Y, PH>(prm, blocks, s); break;
+        case 8: dslash_go<P, NL, EPI_AXPY, DOT_SELF, PH>(prm, blocks, s); break;
+    }
+}
+
+// The reduced-precision sweeps (issue-bound) get code specialised to the phase
+// pattern; FP64 (bandwidth-bound) decides per launch.
 template <int P, int NL>
 static void dslash_dispatch(const DslashParams<P>& prm, int epi, int dot, int blocks, cudaStream_t s)
 {
-    switch (epi * 3 + dot) {
-        case 0: dslash_go<P, NL, EPI_PLAIN, DOT_NONE>(prm, blocks, s); break;
-        case 1: dslash_go<P, NL, EPI_PLAIN, DOT_Y>(prm, blocks, s); break;
-        case 2: dslash_go<P, NL, EPI_PLAIN, DOT_SELF>(prm, blocks, s); break;
-        case 3: dslash_go<P, NL, EPI_DIAG, DOT_NONE>(prm, blocks, s); break;
-        case 4: dslash_go<P, NL, EPI_DIAG, DOT_Y>(prm, blocks, s); break;
-        case 5: dslash_go<P, NL, EPI_DIAG, DOT_SELF>(prm, blocks, s); break;
-        case 6: dslash_go<P, NL, EPI_AXPY, DOT_NONE>(prm, blocks, s); break;
-        case 7: dslash_go<P, NL, EPI_AXPY, DOT_Y>(prm, blocks, s); break;
-        case 8: dslash_go<P, NL, EPI_AXPY, DOT_SELF>(prm, blocks, s); break;
+    if constexpr (P == 64) {
+        dslash_dispatch_ph<P, NL, PH_ANY>(prm, epi, dot, blocks, s);
+    } else {
+        const unsigned m = prm.c.real_mask;
+        if (m == 0xFFu)
+            dslash_dispatch_ph<P, NL, PH_REAL>(prm, epi, dot, blocks, s);
+        else if ((m & 0xFCu) == 0xFCu)
+            dslash_dispatch_ph<P, NL, PH_TCPLX>(prm, epi, dot, blocks, s);
+        else
+            dslash_dispatch_ph<P, NL, PH_ANY>(prm, epi, dot, blocks, s);
     }
 }
 
@@ -625,6 +643,7 @@ C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream)
     chk(cudaMallocHost(&ctx->host_pinned, 64 * sizeof(double)), "cudaMallocHost");
     chk(cudaEventCreate(&ctx->ev0), "cudaEventCreate");
     chk(cudaEventCreate(&ctx->ev1), "cudaEventCreate");
+    for (auto& e : ctx->ring_ev) chk(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     if (rc == C2Q_OK) {
         chk(cudaMemsetAsync(ctx->ticket, 0, 64 * sizeof(unsigned), ctx->stream), "memset");
         chk(cudaMemsetAsync(ctx->scalars, 0, sizeof(SolverScalars), ctx->stream), "memset");
@@ -660,6 +679,8 @@ C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx)
     for (auto e : ctx->event_pool) cudaEventDestroy(e);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    for (auto e : ctx->ring_ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return C2Q_OK;

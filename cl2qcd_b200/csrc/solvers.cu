@@ -187,6 +187,34 @@ void finish_report(c2q_solve_report* rep, int status, int iters, int rel, double
     rep->dslash_applications = sweeps;
 }
 
+// Ring of pinned slots receiving |r|^2 (SolverScalars::resid) and the
+// division flag of each iteration, with one event per slot.
+struct ResidRing {
+    static constexpr int N = 4;
+    c2q_ctx* ctx;
+    explicit ResidRing(c2q_ctx* c) : ctx(c) {}
+    int push(int k)
+    {
+        double* slot = ctx->host_pinned + 32 + 2 * (k % N);
+        C2Q_CUDA(ctx, cudaMemcpyAsync(slot, &ctx->scalars->resid, sizeof(double), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        C2Q_CUDA(ctx, cudaMemcpyAsync(slot + 1, &ctx->scalars->flag, sizeof(int), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[k % N], ctx->stream));
+        return C2Q_OK;
+    }
+    int pop(int k, double* resid, int* flag)
+    {
+        C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[k % N]));
+        const double* slot = ctx->host_pinned + 32 + 2 * (k % N);
+        *resid             = slot[0];
+        int f;
+        memcpy(&f, slot + 1, sizeof(int));
+        *flag = f;
+        return C2Q_OK;
+    }
+};
+
 // ------------------------------------------------------------------ FP64 CG
 // physics/algorithms/solvers/cg.cpp:277-400 with device-resident scalars.
 int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
@@ -212,49 +240,99 @@ int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2
     double resid = std::numeric_limits<double>::quiet_NaN();
     bool force_refresh = false;
     double r2_confirmed = -1.0;  // true residual of the returned solution, when already computed
-    for (iter = 0; iter < P->cgmax || iter < P->min_iter; iter++) {
-        if (iter % P->iter_refresh == 0 || force_refresh) {
-            force_refresh = false;
-            rc = apply_operator(ctx, op, rn, g, gk, x, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
-            if (!rc) rc = saxpy_norm(ctx, rn, Cx{1, 0}, rn, b, FIN_CG_OMEGA, nullptr);  // rn = b - A x ; omega = (rn,rn)
-            if (!rc) rc = copy_field(ctx, p, rn);
+    if (P->rel_tol > 0) {
+        // True-residual target: residual monitored every iteration through the
+        // pinned ring (no host round trip per iteration); a converged iterated
+        // residual is confirmed by an FP64 true residual, else CG restarts from it.
+        ResidRing ring(ctx);
+        int skip_upto = -1;
+        for (iter = 0; iter < P->cgmax || iter < P->min_iter; iter++) {
+            if (iter % P->iter_refresh == 0 || force_refresh) {
+                force_refresh = false;
+                rc = apply_operator(ctx, op, rn, g, gk, x, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
+                if (!rc) rc = saxpy_norm(ctx, rn, Cx{1, 0}, rn, b, FIN_CG_OMEGA, nullptr);
+                if (!rc) rc = copy_field(ctx, p, rn);
+            } else {
+                rc = launch_cg_p(ctx, p, rn);  // p = rn + beta p
+            }
             if (rc) return rc;
-        }
-        DotSpec d;
-        d.mode = DOT_Y;
-        d.y    = p;
-        d.fin  = FIN_CG_ALPHA;  // rho = (p, v) ; alpha = omega / rho
-        rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
-        if (!rc) rc = launch_cg_update(ctx, x, rn, p, v);  // x += alpha p ; rn -= alpha v ; beta, omega
-        if (rc) return rc;
-        if (iter % P->resid_check_every == 0) {
-            SolverScalars h;
-            rc = read_sc(ctx, &h);
+            DotSpec d;
+            d.mode = DOT_Y;
+            d.y    = p;
+            d.fin  = FIN_CG_ALPHA;
+            rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
+            if (!rc) rc = launch_cg_update(ctx, x, rn, p, v);
+            if (!rc) rc = ring.push(iter);
             if (rc) return rc;
-            resid = h.resid;
+            if (iter == 0) continue;
+            double rprev = 0.0;
+            int bad      = 0;
+            rc           = ring.pop(iter - 1, &rprev, &bad);
+            if (rc) return rc;
+            if (iter - 1 <= skip_upto) continue;
+            resid = rprev;
             if (resid != resid) {
                 status = C2Q_SOLVER_STUCK;
                 break;
             }
             if (resid < thr && iter >= P->min_iter) {
-                if (P->rel_tol > 0) {
-                    double r2t = 0;
-                    rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, t2, t1, v, &r2t, &sweeps);
-                    if (rc) return rc;
-                    if (r2t <= P->rel_tol * P->rel_tol * b2 || (P->prec > 0 && r2t < P->prec)) {
-                        status       = iter;
-                        r2_confirmed = r2t;
-                        break;
-                    }
-                    force_refresh = true;  // iterated residual drifted: restart from the true residual
-                    continue;
+                double r2t = 0;
+                rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, t2, t1, v, &r2t, &sweeps);
+                if (rc) return rc;
+                if (r2t <= P->rel_tol * P->rel_tol * b2 || (P->prec > 0 && r2t < P->prec)) {
+                    status       = iter;
+                    r2_confirmed = r2t;
+                    break;
                 }
-                status = iter;
-                break;
+                force_refresh = true;  // the iterated residual drifted: restart from the true residual
+                skip_upto     = iter;
             }
         }
-        rc = launch_cg_p(ctx, p, rn);  // p = rn + beta p
-        if (rc) return rc;
+    } else {
+        for (iter = 0; iter < P->cgmax || iter < P->min_iter; iter++) {
+            if (iter % P->iter_refresh == 0 || force_refresh) {
+                force_refresh = false;
+                rc = apply_operator(ctx, op, rn, g, gk, x, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
+                if (!rc) rc = saxpy_norm(ctx, rn, Cx{1, 0}, rn, b, FIN_CG_OMEGA, nullptr);  // rn = b - A x ; omega = (rn,rn)
+                if (!rc) rc = copy_field(ctx, p, rn);
+                if (rc) return rc;
+            }
+            DotSpec d;
+            d.mode = DOT_Y;
+            d.y    = p;
+            d.fin  = FIN_CG_ALPHA;  // rho = (p, v) ; alpha = omega / rho
+            rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
+            if (!rc) rc = launch_cg_update(ctx, x, rn, p, v);  // x += alpha p ; rn -= alpha v ; beta, omega
+            if (rc) return rc;
+            if (iter % P->resid_check_every == 0) {
+                SolverScalars h;
+                rc = read_sc(ctx, &h);
+                if (rc) return rc;
+                resid = h.resid;
+                if (resid != resid) {
+                    status = C2Q_SOLVER_STUCK;
+                    break;
+                }
+                if (resid < thr && iter >= P->min_iter) {
+                    if (P->rel_tol > 0) {
+                        double r2t = 0;
+                        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, t2, t1, v, &r2t, &sweeps);
+                        if (rc) return rc;
+                        if (r2t <= P->rel_tol * P->rel_tol * b2 || (P->prec > 0 && r2t < P->prec)) {
+                            status       = iter;
+                            r2_confirmed = r2t;
+                            break;
+                        }
+                        force_refresh = true;  // iterated residual drifted: restart from the true residual
+                        continue;
+                    }
+                    status = iter;
+                    break;
+                }
+            }
+            rc = launch_cg_p(ctx, p, rn);  // p = rn + beta p
+            if (rc) return rc;
+        }
     }
     double r2t = r2_confirmed;
     if (r2t < 0) {
@@ -371,52 +449,65 @@ int cg_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c
         if (!rc) rc = write_sc(ctx, s0);
         if (rc) return rc;
         double maxrr = std::sqrt(r2);
+        // Pipelined residual monitoring: every iteration copies |r|^2 into a
+        // pinned ring slot and records an event; the host reads iteration k-1
+        // while iteration k runs, so the GPU never waits for the host.  A
+        // decision taken on iteration k-1 is applied after iteration k.
+        ResidRing ring(ctx);
+        int skip_upto = -1;  // ring entries <= this index predate the last reliable update
         for (iter = 0; iter < P->cgmax; ++iter) {
+            if (iter > 0) {
+                rc = mix_p<PB>(ctx, p, rs);  // p = r + beta p (beta of the previous iteration)
+                if (rc) return rc;
+            }
             DotSpec d;
             d.mode = DOT_Y;
             d.y    = p;
             d.fin  = FIN_CG_ALPHA;
             rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
             if (!rc) rc = mix_update<PB>(ctx, xs, rs, p, v);
+            if (!rc) rc = ring.push(iter);
             if (rc) return rc;
-            if (iter % P->resid_check_every == 0) {
+            if (iter == 0) continue;
+            double rprev = 0.0;
+            int bad      = 0;
+            rc           = ring.pop(iter - 1, &rprev, &bad);
+            if (rc) return rc;
+            if (iter - 1 <= skip_upto) continue;
+            resid = rprev;
+            if (resid != resid || bad) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            const double rn = std::sqrt(resid);
+            if (rn > maxrr) maxrr = rn;
+            if (rn < delta * maxrr || resid < thr) {
+                // reliable update in FP64 after iteration `iter`
                 SolverScalars h;
-                rc = read_sc(ctx, &h);
+                rc = read_sc(ctx, &h);  // scalars of iteration `iter`
+                if (!rc) rc = accumulate(ctx, x, xs);
+                if (!rc) rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
                 if (rc) return rc;
-                resid = h.resid;
-                if (resid != resid || h.flag) {
-                    status = C2Q_SOLVER_STUCK;
+                ++reliable;
+                resid = r2;
+                if (r2 < thr) {
+                    status       = iter + 1;
+                    r2_confirmed = r2;
                     break;
                 }
-                const double rn = std::sqrt(resid);
-                if (rn > maxrr) maxrr = rn;
-                if (rn < delta * maxrr || resid < thr) {
-                    // reliable update in FP64
-                    rc = accumulate(ctx, x, xs);
-                    if (!rc) rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
-                    if (rc) return rc;
-                    ++reliable;
-                    resid = r2;
-                    if (r2 < thr) {
-                        status       = iter + 1;
-                        r2_confirmed = r2;
-                        break;
-                    }
-                    rc = launch_convert(ctx, rs, r64);
-                    if (rc) return rc;
-                    maxrr = std::sqrt(r2);
-                    // keep the search direction; rescale beta to the true residual
-                    h.beta[0] *= r2 / h.resid;
-                    h.beta[1] *= r2 / h.resid;
-                    h.omega[0] = r2;
-                    h.omega[1] = 0.0;
-                    h.resid    = r2;
-                    rc         = write_sc(ctx, h);
-                    if (rc) return rc;
-                }
+                rc = launch_convert(ctx, rs, r64);
+                if (rc) return rc;
+                maxrr = std::sqrt(r2);
+                // keep the search direction; rescale beta to the true residual
+                h.beta[0] *= r2 / h.resid;
+                h.beta[1] *= r2 / h.resid;
+                h.omega[0] = r2;
+                h.omega[1] = 0.0;
+                h.resid    = r2;
+                rc         = write_sc(ctx, h);
+                if (rc) return rc;
+                skip_upto = iter;
             }
-            rc = mix_p<PB>(ctx, p, rs);
-            if (rc) return rc;
         }
         if (status == C2Q_DID_NOT_SOLVE || status == C2Q_SOLVER_STUCK) {
             // keep what was gained
@@ -636,7 +727,7 @@ C2Q_EXPORT void c2q_solver_params_default(c2q_solver_params* p)
     p->resid_check_every = 10;                   // :87
     p->min_iter          = 0;
     p->precision         = C2Q_PREC_FP64;
-    p->reliable_delta    = 0.1;
+    p->reliable_delta    = 0.01;
     p->use_rec12         = 0;
     p->use_graph         = 0;
 }

@@ -130,3 +130,33 @@ def test_perform_inversion_matches_oracle(port, system, O, solver):
     assert rel_l2(out, ref) < 1e-9
     # the reference's eo inversion returns -M^{-1} b
     assert rel_l2(port.m_tm_plus(-out, g, kappa, mubar), src) < 1e-9
+
+
+@pytest.mark.parametrize("bc", [(0.0, 0.0, None, None), (1.0, 0.0, None, None), (1.0, 0.5, None, 0.1)])
+@pytest.mark.parametrize("precision", [32, 16])
+def test_mixed_cg_all_phase_patterns(port, system, O, bc, precision):
+    """The reduced-precision sweeps are specialised for all-real phases, complex T
+    phases only, and general phases; each must drive the mixed CG to 1e-10 in about
+    as many iterations as FP64 (a wrong inner operator would not converge).  The
+    general case uses a spatial phase and an imaginary chemical potential: a real
+    chemical potential breaks the gamma5-hermiticity that CG on QplusQminus_eo needs."""
+    import cl2qcd_b200 as c2q
+    tt, ts, cpr, cpi = bc
+    port.set_lattice(8, 8, tt, ts, cpr, cpi)
+    L = c2q.Lattice(8, 8, tt, ts, cpr, cpi)
+    g = c2q.host.generate_gaugefield(L, 0.3, 9)
+    gf = c2q.Gaugefield(system, L, g)
+    b = c2q.host.generate_source(port.seo, "gaussian", 10)
+    add = c2q.AdditionalParameters(0.14, 2 * 0.14 * 0.02)
+    B = c2q.Spinorfield_eo(system, L, b)
+    reps = {}
+    for prec in (64, precision):
+        X = c2q.Spinorfield_eo(system, L)
+        reps[prec] = {}
+        c2q.host.cg(X, c2q.host.QplusQminus_eo(), gf, B,
+                    c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=1e-10, cgmax=5000, precision=prec,
+                                         use_rec12=True), add, reps[prec])
+        assert reps[prec]["true_resid_rel"] <= 1e-10
+        r = port.apply(O.OP_QPQM_EO, X.dump(), g, add.kappa, add.mubar)
+        assert np.linalg.norm(r - b) / np.linalg.norm(b) <= 1.5e-10
+    assert reps[precision]["iterations"] <= 1.3 * reps[64]["iterations"] + 10
