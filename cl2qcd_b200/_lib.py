@@ -65,6 +65,10 @@ SIGNATURES = {
     "c2q_gauge_destroy": (C.c_int, [_P]),
     "c2q_gauge_device_bytes": (C.c_size_t, [_P]),
     "c2q_spinor_eo_create": (C.c_int, [_P, C.POINTER(CLattice), C.POINTER(_P)]),
+    "c2q_spinor_eo_create_precision": (C.c_int, [_P, C.POINTER(CLattice), C.c_int, C.POINTER(_P)]),
+    "c2q_spinor_eo_precision": (C.c_int, [_P]),
+    "c2q_spinor_eo_convert": (C.c_int, [_P, _P]),
+    "c2q_ctx_set_link_format": (C.c_int, [_P, C.c_int]),
     "c2q_spinor_eo_destroy": (C.c_int, [_P]),
     "c2q_spinor_eo_upload": (C.c_int, [_P, _D]),
     "c2q_spinor_eo_download": (C.c_int, [_P, _D]),

@@ -10,6 +10,8 @@
 
 #include "../../include/cl2qcd_b200.h"
 #include "c2q_internal.cuh"
+#include "blas.cuh"
+#include "pack.cuh"
 #include "reduce.cuh"
 
 namespace c2q {
@@ -52,6 +54,8 @@ struct c2q_ctx {
     };
     std::vector<Timed> timed;
     std::vector<cudaEvent_t> event_pool;
+    // link storage of the explicit operator entry points: 0 18-real, 1 12-real
+    int rec12 = 0;
 };
 
 struct c2q_gauge {
@@ -92,6 +96,9 @@ bool same_lattice(const c2q_lattice& a, const c2q_lattice& b);
 HopCoef hop_coef(const c2q_lattice& lat, double kappa);
 EpiArgs diag_epi(double mubar, int which, int gamma5);
 
+// gauge storage for operator sweeps at precision `prec` (FP16 links are always 12-real)
+int gkind_for(int prec, int rec12);
+
 // ---- fields ----
 // Allocate a spinor field of storage precision `prec` (stream-ordered allocation).
 int field_alloc(c2q_ctx* ctx, const c2q_lattice& lat, int prec, c2q_spinor_eo* f);
@@ -104,7 +111,7 @@ int ensure_partials(c2q_ctx* ctx, size_t blocks);
 template <int P>
 inline SpinorPtr<P> sptr(const c2q_spinor_eo* f)
 {
-    return SpinorPtr<P>{f ? f->data : nullptr, f ? f->norm : nullptr};
+    return SpinorPtr<P>{f ? f->data : nullptr, f ? f->norm : nullptr, f ? f->geom.seo / 2 : 0};
 }
 
 // ---- launches (all stream-ordered on ctx->stream) ----
@@ -131,6 +138,29 @@ int launch_cg_update(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* r, const c2q
                      const c2q_spinor_eo* v);
 int launch_cg_p(c2q_ctx* ctx, c2q_spinor_eo* p, const c2q_spinor_eo* r);
 int launch_convert(c2q_ctx* ctx, c2q_spinor_eo* out, const c2q_spinor_eo* in);
+
+// A batch of right-hand sides for one sweep of the paired-site dslash
+// (FP32 / FP16 fields, pdslash.cuh): per right-hand side r, out[r] = epilogue
+// of the hopping term on in[r], with x[r] the EPI_AXPY operand, y[r] the DOT_Y
+// partner and sc[r] the solver scalars its reduction finishes into.
+constexpr int MAX_BATCH = PK_MAX_RHS;
+struct PkBatch {
+    int n = 0;
+    c2q_spinor_eo* out[MAX_BATCH] = {};
+    const c2q_spinor_eo* in[MAX_BATCH] = {};
+    const c2q_spinor_eo* x[MAX_BATCH] = {};
+    const c2q_spinor_eo* y[MAX_BATCH] = {};
+    SolverScalars* sc[MAX_BATCH] = {};
+    int out_parity = 0;
+    double kappa = 0;
+    int epi = 0;
+    EpiArgs e{1, 0, 1, 0, 0};
+    int dot_mode = 0;
+    int fin = FIN_STORE_RESULT;
+};
+int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B);
+// an event for per-launch profiling (from the context's pool)
+cudaEvent_t profile_event(c2q_ctx* ctx);
 
 // Fermion matrix application at the fields' precision.  tmp1/tmp2 are
 // scratch fields of the same precision.  `dot` applies to the last sweep.

@@ -9,9 +9,9 @@
 //     for every lane in every precision), so a warp reads 32 consecutive sites
 //     of one lane with one 128-bit (FP64, FP32) or 64/128-bit (FP16) load each;
 //   * FP64 spinor: 12 double2 lanes (spin-major: k = 3*spin + colour);
-//     FP32 spinor: 6 float4 lanes (complex 2k, 2k+1 in lane k);
-//     FP16 spinor: 3 int4 lanes of 8 int16 fixed-point values each, scaled by a
-//       per-site float norm (max |component|) held in a separate float array;
+//     FP32 and FP16 spinors (and their links) pair the sites i and i + Seo/2
+//     in one "slot" (pack.cuh): FP32 12 float4 lanes, FP16 6 uint4 lanes of
+//     16-bit fixed point with a per-site float norm (max |component|);
 //   * gauge field: links are grouped by the parity of the site they start at,
 //     [parity][mu][lane][stride], so the 4 forward links of an output site and
 //     the 4 backward links (which start at opposite-parity neighbours) are both
@@ -146,6 +146,7 @@ template <int P>
 struct SpinorPtr {
     void* data;    // lanes
     float* norm;   // FP16 only: per-site scale
+    int half = 0;  // FP32 / FP16: H = Seo/2, the number of site pairs (slots)
 };
 
 template <int P>
@@ -171,25 +172,39 @@ struct SpinorIO<64> {
     }
 };
 
+// Per-site access to the paired-site ("slot") layout of the FP32 and FP16
+// fields (pack.cuh): eo site i is half h = (i >= H) of slot j = i - h H, and
+// its two words sit at offset h inside each pair.  The hot kernels work on
+// whole slots; these accessors serve conversions and the generic BLAS.
+__device__ __forceinline__ int slot_of(int i, int half, int* h)
+{
+    *h = i >= half;
+    return i - (*h) * half;
+}
+
 template <>
 struct SpinorIO<32> {
     using R = float;
     static __device__ __forceinline__ void load(const SpinorPtr<32>& f, int stride, int i, Cplx<R> s[12])
     {
-        const float4* p = static_cast<const float4*>(f.data);
+        int h;
+        const int j     = slot_of(i, f.half, &h);
+        const float* p  = static_cast<const float*>(f.data) + (size_t)j * 4 + h;
+        const size_t ls = (size_t)(stride >> 1) * 4;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            float4 v     = __ldg(p + (size_t)k * stride + i);
-            s[2 * k]     = {v.x, v.y};
-            s[2 * k + 1] = {v.z, v.w};
-        }
+        for (int k = 0; k < 12; ++k) s[k] = {__ldg(p + k * ls), __ldg(p + k * ls + 2)};
     }
     static __device__ __forceinline__ void store(const SpinorPtr<32>& f, int stride, int i, const Cplx<R> s[12])
     {
-        float4* p = static_cast<float4*>(f.data);
+        int h;
+        const int j     = slot_of(i, f.half, &h);
+        float* p        = static_cast<float*>(f.data) + (size_t)j * 4 + h;
+        const size_t ls = (size_t)(stride >> 1) * 4;
 #pragma unroll
-        for (int k = 0; k < 6; ++k)
-            p[(size_t)k * stride + i] = make_float4(s[2 * k].re, s[2 * k].im, s[2 * k + 1].re, s[2 * k + 1].im);
+        for (int k = 0; k < 12; ++k) {
+            p[k * ls]     = s[k].re;
+            p[k * ls + 2] = s[k].im;
+        }
     }
 };
 
@@ -216,28 +231,19 @@ __device__ __forceinline__ unsigned eq_pair(float re, float im, float inv)
 template <>
 struct SpinorIO<16> {
     using R = float;
-    // raw words (complex k in word k: re low half, im high half) and the scale norm/32767
-    static __device__ __forceinline__ void load_raw(const SpinorPtr<16>& f, int stride, int i, unsigned w[12],
-                                                    float* sc)
-    {
-        const uint4* p = static_cast<const uint4*>(f.data);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const uint4 v = __ldg(p + (size_t)k * stride + i);
-            w[4 * k]      = v.x;
-            w[4 * k + 1]  = v.y;
-            w[4 * k + 2]  = v.z;
-            w[4 * k + 3]  = v.w;
-        }
-        *sc = __ldg(f.norm + i) * (1.0f / 32767.0f);
-    }
+    // word of component k of (slot j, half h): lane k/2, position 2 (k & 1) + h
     static __device__ __forceinline__ void load(const SpinorPtr<16>& f, int stride, int i, Cplx<R> s[12])
     {
-        unsigned w[12];
-        float sc;
-        load_raw(f, stride, i, w, &sc);
+        int h;
+        const int j       = slot_of(i, f.half, &h);
+        const unsigned* p = static_cast<const unsigned*>(f.data) + (size_t)j * 4 + h;
+        const size_t ls   = (size_t)(stride >> 1) * 4;
+        const float sc    = __ldg(f.norm + 2 * j + h) * (1.0f / 32767.0f);
 #pragma unroll
-        for (int k = 0; k < 12; ++k) s[k] = {sc * dq_lo(w[k]), sc * dq_hi(w[k])};
+        for (int k = 0; k < 12; ++k) {
+            const unsigned w = __ldg(p + (k >> 1) * ls + 2 * (k & 1));
+            s[k]             = {sc * dq_lo(w), sc * dq_hi(w)};
+        }
     }
     static __device__ __forceinline__ void store(const SpinorPtr<16>& f, int stride, int i, const Cplx<R> s[12])
     {
@@ -245,19 +251,18 @@ struct SpinorIO<16> {
 #pragma unroll
         for (int k = 0; k < 12; ++k) mx = fmaxf(mx, fmaxf(fabsf(s[k].re), fabsf(s[k].im)));
         const float inv = mx > 0.f ? 32767.0f / mx : 0.f;
-        uint4* p        = static_cast<uint4*>(f.data);
+        int h;
+        const int j     = slot_of(i, f.half, &h);
+        unsigned* p     = static_cast<unsigned*>(f.data) + (size_t)j * 4 + h;
+        const size_t ls = (size_t)(stride >> 1) * 4;
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
-            p[(size_t)k * stride + i] = make_uint4(eq_pair(s[4 * k].re, s[4 * k].im, inv),
-                                                   eq_pair(s[4 * k + 1].re, s[4 * k + 1].im, inv),
-                                                   eq_pair(s[4 * k + 2].re, s[4 * k + 2].im, inv),
-                                                   eq_pair(s[4 * k + 3].re, s[4 * k + 3].im, inv));
-        f.norm[i] = mx;
+        for (int k = 0; k < 12; ++k) p[(k >> 1) * ls + 2 * (k & 1)] = eq_pair(s[k].re, s[k].im, inv);
+        f.norm[2 * j + h] = mx;
     }
 };
 
 // ------------------------------------------------------------------------
-// gauge links: NL = 9 (18-real) or 6 (12-real) complex lanes per link.
+// FP64 gauge links: NL = 9 (18-real) or 6 (12-real) complex lanes per link.
 // ------------------------------------------------------------------------
 template <int P, int NL>
 struct LinkIO;
@@ -272,40 +277,6 @@ struct LinkIO<64, NL> {
         for (int k = 0; k < NL; ++k) {
             double2 v = __ldg(p + k * lane_stride + idx);
             u[k]      = {v.x, v.y};
-        }
-    }
-};
-
-template <int NL>
-struct LinkIO<32, NL> {
-    using R = float;
-    static __device__ __forceinline__ void load(const void* base, size_t lane_stride, size_t idx, Cplx<R> u[9])
-    {
-        const float2* p = static_cast<const float2*>(base);
-#pragma unroll
-        for (int k = 0; k < NL; ++k) {
-            float2 v = __ldg(p + k * lane_stride + idx);
-            u[k]     = {v.x, v.y};
-        }
-    }
-};
-
-// FP16 links: 12-real only.  Entries of an SU(3) matrix are bounded by 1, so
-// a fixed scale is used: u = q + 32768, q = rint(v * 32767) (same biased
-// encoding as the spinors).  Rows 0 and 1 are three uint2 lanes (complex 2j,
-// 2j+1 in lane j).  load_q returns the entries in units of 1/32767.
-template <int NL>
-struct LinkIO<16, NL> {
-    static_assert(NL == 6, "FP16 links are stored 12-real");
-    using R = float;
-    static __device__ __forceinline__ void load_q(const void* base, size_t lane_stride, size_t idx, Cplx<R> u[9])
-    {
-        const uint2* p = static_cast<const uint2*>(base);
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const uint2 v = __ldg(p + j * lane_stride + idx);
-            u[2 * j]      = {dq_lo(v.x), dq_hi(v.x)};
-            u[2 * j + 1]  = {dq_lo(v.y), dq_hi(v.y)};
         }
     }
 };

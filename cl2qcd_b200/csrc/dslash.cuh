@@ -1,5 +1,6 @@
 // dslash.cuh -- the even-odd Wilson hopping term with fused twisted-mass
-// epilogues, for one output parity, one thread per output site.
+// epilogues, for one output parity, one thread per output site, on the FP64
+// fields (the FP32 / FP16 fields use the paired-site kernel of pdslash.cuh).
 //
 // Computes, at every site x of the output parity,
 //   h(x) = sum_mu [ c_mu^+ (1 - g_mu) U_mu(x) psi(x+mu)
@@ -119,18 +120,6 @@ __device__ __forceinline__ void project(Cplx<R> h[3], const Cplx<R> psi[12])
 #pragma unroll
     for (int col = 0; col < 3; ++col) h[col] = psi[3 * A + col] + mul_unit<CK>(psi[3 * PP + col]);
 }
-// Same from FP16 raw words (values in units of the site's scale).
-template <int A, int PP, int CK>
-__device__ __forceinline__ void project_raw(Cplx<float> h[3], const unsigned w[12])
-{
-#pragma unroll
-    for (int col = 0; col < 3; ++col) {
-        const Cplx<float> a = {dq_lo(w[3 * A + col]), dq_hi(w[3 * A + col])};
-        const Cplx<float> b = {dq_lo(w[3 * PP + col]), dq_hi(w[3 * PP + col])};
-        h[col]              = a + mul_unit<CK>(b);
-    }
-}
-
 template <typename R, int MU, bool BACK, bool KREAL>
 __device__ __forceinline__ void hop_decoded(Cplx<R> acc[12], const Cplx<R> psi[12], const Cplx<R> u[9], Cplx<R> k)
 {
@@ -142,20 +131,6 @@ __device__ __forceinline__ void hop_decoded(Cplx<R> acc[12], const Cplx<R> psi[1
     hop_channel<R, 0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
     project<R, 1, T::p1, c1>(h, psi);
     hop_channel<R, 1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
-}
-
-template <int MU, bool BACK, bool KREAL>
-__device__ __forceinline__ void hop_raw(Cplx<float> acc[12], const unsigned w[12], const Cplx<float> u[9],
-                                        Cplx<float> k)
-{
-    using T          = Proj<MU>;
-    constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
-    constexpr int c1 = BACK ? NegUnit<T::c1>::value : T::c1;
-    Cplx<float> h[3];
-    project_raw<0, T::p0, c0>(h, w);
-    hop_channel<float, 0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
-    project_raw<1, T::p1, c1>(h, w);
-    hop_channel<float, 1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
 }
 
 // Phase patterns known at compile time (the common boundary conditions): PH_REAL
@@ -176,28 +151,15 @@ __device__ __forceinline__ void do_hop(Cplx<typename Prec<P>::R> acc[12], const 
                        : PH == PH_TCPLX ? (MU != 0)
                                         : (bool)((prm.c.real_mask >> (2 * MU + d)) & 1u);
     Cplx<R> u[9];
-    if constexpr (P == 16) {
-        unsigned w[12];
-        float sc;
-        SpinorIO<16>::load_raw(prm.in, g.stride, i_nb, w, &sc);
-        LinkIO<16, NL>::load_q(links, ls, link_idx, u);
-        reconstruct_row2(u, 1.0f / 32767.0f);
-        const Cplx<float> k = {(float)prm.c.re[MU][d] * sc, (float)prm.c.im[MU][d] * sc};
-        if (kreal)
-            hop_raw<MU, BACK, true>(acc, w, u, k);
-        else
-            hop_raw<MU, BACK, false>(acc, w, u, k);
-    } else {
-        Cplx<R> psi[12];
-        SpinorIO<P>::load(prm.in, g.stride, i_nb, psi);
-        LinkIO<P, NL>::load(links, ls, link_idx, u);
-        if (NL == 6) reconstruct_row2(u);
-        const Cplx<R> k = cmk<R>((R)prm.c.re[MU][d], (R)prm.c.im[MU][d]);
-        if (kreal)
-            hop_decoded<R, MU, BACK, true>(acc, psi, u, k);
-        else
-            hop_decoded<R, MU, BACK, false>(acc, psi, u, k);
-    }
+    Cplx<R> psi[12];
+    SpinorIO<P>::load(prm.in, g.stride, i_nb, psi);
+    LinkIO<P, NL>::load(links, ls, link_idx, u);
+    if (NL == 6) reconstruct_row2(u);
+    const Cplx<R> k = cmk<R>((R)prm.c.re[MU][d], (R)prm.c.im[MU][d]);
+    if (kreal)
+        hop_decoded<R, MU, BACK, true>(acc, psi, u, k);
+    else
+        hop_decoded<R, MU, BACK, false>(acc, psi, u, k);
 }
 
 template <int P, int NL, int MU, int PH>
@@ -206,8 +168,7 @@ __device__ __forceinline__ void do_direction(Cplx<typename Prec<P>::R> acc[12], 
 {
     const size_t ls       = (size_t)prm.g.stride;
     const int po          = prm.out_parity;
-    // element size of one complex lane entry in this precision
-    constexpr size_t esz  = P == 64 ? 16 : (P == 32 ? 8 : 4);
+    constexpr size_t esz  = 16;  // one double2 per complex lane entry
     const char* gbase     = static_cast<const char*>(prm.gauge);
     const char* fwd_links = gbase + (size_t)((po * 4 + MU) * NL) * ls * esz;
     const char* bwd_links = gbase + (size_t)(((1 - po) * 4 + MU) * NL) * ls * esz;
@@ -216,7 +177,7 @@ __device__ __forceinline__ void do_direction(Cplx<typename Prec<P>::R> acc[12], 
 }
 
 template <int P, int NL, int EPI, int DOT, int PH>
-__global__ void __launch_bounds__(128, P == 16 ? 7 : 1) dslash_kernel(const DslashParams<P> prm)
+__global__ void __launch_bounds__(128) dslash_kernel(const DslashParams<P> prm)
 {
     using R       = typename Prec<P>::R;
     const Geom& g = prm.g;

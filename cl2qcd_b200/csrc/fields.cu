@@ -124,6 +124,8 @@ int field_alloc(c2q_ctx* ctx, const c2q_lattice& lat, int prec, c2q_spinor_eo* f
     f->lat  = lat;
     f->prec = prec;
     if (!make_geom(lat, &f->geom)) return fail(ctx, C2Q_BAD_ARG, "lattice extents must be even and >= 2");
+    if (prec != 64 && (lat.nt % 4))
+        return fail(ctx, C2Q_BAD_ARG, "FP32 / FP16 fields pair the times t and t + NT/2: NT must be a multiple of 4");
     const size_t bytes = field_bytes(f->geom, prec);
     void* p            = nullptr;
     C2Q_CUDA(ctx, cudaMallocAsync(&p, bytes, ctx->stream));
@@ -139,6 +141,25 @@ void field_free(c2q_spinor_eo* f)
 {
     if (f && f->data && f->owned) cudaFreeAsync(f->data, f->ctx->stream);
     if (f) f->data = nullptr;
+}
+
+int gkind_for(int prec, int rec12)
+{
+    if (prec == 64) return rec12 ? G64R12 : G64;
+    if (prec == 32) return rec12 ? G32R12 : G32;
+    return G16R12;
+}
+
+cudaEvent_t profile_event(c2q_ctx* ctx)
+{
+    cudaEvent_t e;
+    if (!ctx->event_pool.empty()) {
+        e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+    } else {
+        cudaEventCreate(&e);
+    }
+    return e;
 }
 
 int ensure_staging(c2q_ctx* ctx, size_t bytes)
@@ -226,28 +247,40 @@ __global__ void gauge_export_kernel(double2* __restrict__ aos, const double2* __
     for (int k = 0; k < 9; ++k) m[k] = src[(size_t)k * g.stride];
 }
 
-// FP64 9-lane store -> other precision / compression (NL lanes).
-template <typename T, int NL>
-__global__ void gauge_convert_kernel(const double2* __restrict__ in, T* __restrict__ out, Geom g)
+// FP64 9-lane store -> FP64 12-real (first NL lanes, same layout).
+__global__ void gauge_convert64_kernel(const double2* __restrict__ in, double2* __restrict__ out, Geom g)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 8LL * g.stride) return;
     const int blk = (int)(t / g.stride), i = (int)(t - (long long)blk * g.stride);  // blk = parity*4 + mu
     const double2* src = in + (size_t)blk * 9 * g.stride + i;
-    T* dst             = out + (size_t)blk * NL * g.stride + i;
+    double2* dst       = out + (size_t)blk * 6 * g.stride + i;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) dst[(size_t)k * g.stride] = src[(size_t)k * g.stride];
+}
+
+// FP64 9-lane store -> FP32 slot layout (pack.cuh): the links of the sites
+// j and j + H of each (parity, mu) group side by side, NL float4 lanes.
+template <int NL>
+__global__ void gauge_convert32_kernel(const double2* __restrict__ in, float4* __restrict__ out, Geom g)
+{
+    const int ss = g.stride / 2, H = g.seo / 2;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 8LL * ss) return;
+    const int blk = (int)(t / ss), j = (int)(t - (long long)blk * ss);
+    if (j >= H) return;
+    const double2* src = in + (size_t)blk * 9 * g.stride;
+    float4* dst        = out + (size_t)blk * NL * ss + j;
 #pragma unroll
     for (int k = 0; k < NL; ++k) {
-        const double2 v = src[(size_t)k * g.stride];
-        if constexpr (sizeof(T) == 16) {
-            dst[(size_t)k * g.stride] = v;
-        } else if constexpr (sizeof(T) == 8) {
-            dst[(size_t)k * g.stride] = T{(float)v.x, (float)v.y};
-        }
+        const double2 a = src[(size_t)k * g.stride + j], b = src[(size_t)k * g.stride + j + H];
+        dst[(size_t)k * ss] = make_float4((float)a.x, (float)b.x, (float)a.y, (float)b.y);
     }
 }
 
-// FP64 9-lane store -> FP16 12-real: rows 0 and 1 as three uint2 lanes of
-// biased 16-bit fixed point (u = rint(v * 32767) + 32768, v clamped to [-1, 1]).
+// FP64 9-lane store -> FP16 12-real slot layout: rows 0 and 1 as biased
+// 16-bit fixed point (u = rint(v * 32767) + 32768, v clamped to [-1, 1]),
+// three uint4 lanes (entry 2L of both sites, entry 2L+1 of both sites).
 __device__ __forceinline__ unsigned enc16(double2 v)
 {
     const double cx = fmin(1.0, fmax(-1.0, v.x)), cy = fmin(1.0, fmax(-1.0, v.y));
@@ -255,17 +288,21 @@ __device__ __forceinline__ unsigned enc16(double2 v)
     const int hi    = __double2int_rn(cy * 32767.0) + 32768;
     return (unsigned)(lo & 0xffff) | ((unsigned)hi << 16);
 }
-__global__ void gauge_convert16_kernel(const double2* __restrict__ in, uint2* __restrict__ out, Geom g)
+__global__ void gauge_convert16_kernel(const double2* __restrict__ in, uint4* __restrict__ out, Geom g)
 {
+    const int ss = g.stride / 2, H = g.seo / 2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 8LL * g.stride) return;
-    const int blk = (int)(t / g.stride), i = (int)(t - (long long)blk * g.stride);
-    const double2* src = in + (size_t)blk * 9 * g.stride + i;
-    uint2* dst         = out + (size_t)blk * 3 * g.stride + i;
+    if (t >= 8LL * ss) return;
+    const int blk = (int)(t / ss), j = (int)(t - (long long)blk * ss);
+    if (j >= H) return;
+    const double2* src = in + (size_t)blk * 9 * g.stride;
+    uint4* dst         = out + (size_t)blk * 3 * ss + j;
 #pragma unroll
-    for (int j = 0; j < 3; ++j)
-        dst[(size_t)j * g.stride] = make_uint2(enc16(src[(size_t)(2 * j) * g.stride]),
-                                               enc16(src[(size_t)(2 * j + 1) * g.stride]));
+    for (int L = 0; L < 3; ++L) {
+        const size_t e0 = (size_t)(2 * L) * g.stride, e1 = (size_t)(2 * L + 1) * g.stride;
+        dst[(size_t)L * ss] = make_uint4(enc16(src[e0 + j]), enc16(src[e0 + j + H]), enc16(src[e1 + j]),
+                                         enc16(src[e1 + j + H]));
+    }
 }
 
 int gauge_ensure(c2q_gauge* g, int kind)
@@ -287,11 +324,15 @@ int gauge_ensure(c2q_gauge* g, int kind)
     const int threads = 256;
     const unsigned blocks = (unsigned)((lanes + threads - 1) / threads);
     const double2* src    = static_cast<const double2*>(g->store[G64].data);
+    if (kind != G64R12 && (g->lat.nt % 4)) {
+        cudaFree(p);
+        return fail(ctx, C2Q_BAD_ARG, "FP32 / FP16 links pair the times t and t + NT/2: NT must be a multiple of 4");
+    }
     switch (kind) {
-        case G64R12: gauge_convert_kernel<double2, 6><<<blocks, threads, 0, ctx->stream>>>(src, (double2*)p, g->geom); break;
-        case G32: gauge_convert_kernel<float2, 9><<<blocks, threads, 0, ctx->stream>>>(src, (float2*)p, g->geom); break;
-        case G32R12: gauge_convert_kernel<float2, 6><<<blocks, threads, 0, ctx->stream>>>(src, (float2*)p, g->geom); break;
-        case G16R12: gauge_convert16_kernel<<<blocks, threads, 0, ctx->stream>>>(src, (uint2*)p, g->geom); break;
+        case G64R12: gauge_convert64_kernel<<<blocks, threads, 0, ctx->stream>>>(src, (double2*)p, g->geom); break;
+        case G32: gauge_convert32_kernel<9><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
+        case G32R12: gauge_convert32_kernel<6><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
+        case G16R12: gauge_convert16_kernel<<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
     }
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
@@ -323,22 +364,11 @@ static void dslash_dispatch_ph(const DslashParams<P>& prm, int epi, int dot, int
     }
 }
 
-// The reduced-precision sweeps (issue-bound) get code specialised to the phase
-// pattern; FP64 (bandwidth-bound) decides per launch.
+// FP64 (bandwidth-bound) decides the phase pattern per launch.
 template <int P, int NL>
 static void dslash_dispatch(const DslashParams<P>& prm, int epi, int dot, int blocks, cudaStream_t s)
 {
-    if constexpr (P == 64) {
-        dslash_dispatch_ph<P, NL, PH_ANY>(prm, epi, dot, blocks, s);
-    } else {
-        const unsigned m = prm.c.real_mask;
-        if (m == 0xFFu)
-            dslash_dispatch_ph<P, NL, PH_REAL>(prm, epi, dot, blocks, s);
-        else if ((m & 0xFCu) == 0xFCu)
-            dslash_dispatch_ph<P, NL, PH_TCPLX>(prm, epi, dot, blocks, s);
-        else
-            dslash_dispatch_ph<P, NL, PH_ANY>(prm, epi, dot, blocks, s);
-    }
+    dslash_dispatch_ph<P, NL, PH_ANY>(prm, epi, dot, blocks, s);
 }
 
 template <int P>
@@ -354,7 +384,6 @@ static int dslash_typed(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_
     prm.gauge      = g->store[gkind].data;
     prm.g          = out->geom;
     prm.c          = hop_coef(out->lat, kappa);
-    if (P == 16) prm.c.scale *= 1.0 / 32767.0;  // FP16 links are applied in units of 1/32767
     prm.e          = e;
     prm.out_parity = out_parity;
     const int blocks = (out->geom.seo + 127) / 128;
@@ -366,36 +395,22 @@ static int dslash_typed(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_
     const bool r12 = gkind == G64R12 || gkind == G32R12 || gkind == G16R12;
     c2q_ctx::Timed tm{};
     if (ctx->profiling) {
-        auto get = [&]() {
-            cudaEvent_t e;
-            if (!ctx->event_pool.empty()) {
-                e = ctx->event_pool.back();
-                ctx->event_pool.pop_back();
-            } else {
-                cudaEventCreate(&e);
-            }
-            return e;
-        };
-        tm.a     = get();
-        tm.b     = get();
+        tm.a     = profile_event(ctx);
+        tm.b     = profile_event(ctx);
         tm.prec  = P;
         tm.sites = (double)out->geom.seo;
         // compulsory traffic per output site: 8 links (each read once per sweep),
         // the input spinor (each read once through L2 reuse), the output, plus
         // the epilogue/reduction operands read at the output site
-        const double sp = P == 64 ? 192.0 : (P == 32 ? 96.0 : 52.0);
-        const double lk = (r12 ? 12.0 : 18.0) * (P == 64 ? 8.0 : (P == 32 ? 4.0 : 2.0));
+        const double sp = 192.0;
+        const double lk = (r12 ? 12.0 : 18.0) * 8.0;
         tm.bytes = tm.sites * (8.0 * lk + sp * (2.0 + (epi == EPI_AXPY ? 1.0 : 0.0) + (dot.mode == DOT_Y ? 1.0 : 0.0)));
         cudaEventRecord(tm.a, ctx->stream);
     }
-    if constexpr (P == 16) {
-        dslash_dispatch<16, 6>(prm, epi, dot.mode, blocks, ctx->stream);
-    } else {
-        if (r12)
-            dslash_dispatch<P, 6>(prm, epi, dot.mode, blocks, ctx->stream);
-        else
-            dslash_dispatch<P, 9>(prm, epi, dot.mode, blocks, ctx->stream);
-    }
+    if (r12)
+        dslash_dispatch<P, 6>(prm, epi, dot.mode, blocks, ctx->stream);
+    else
+        dslash_dispatch<P, 9>(prm, epi, dot.mode, blocks, ctx->stream);
     if (ctx->profiling) {
         cudaEventRecord(tm.b, ctx->stream);
         ctx->timed.push_back(tm);
@@ -425,11 +440,20 @@ int launch_dslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_eo* ou
     if (!gauge_matches(out->prec, gkind)) return fail(ctx, C2Q_BAD_ARG, "gauge precision mismatch");
     int rc = gauge_ensure(const_cast<c2q_gauge*>(g), gkind);
     if (rc) return rc;
-    switch (out->prec) {
-        case 64: return dslash_typed<64>(ctx, g, gkind, out, in, out_parity, kappa, epi, e, x, dot);
-        case 32: return dslash_typed<32>(ctx, g, gkind, out, in, out_parity, kappa, epi, e, x, dot);
-        default: return dslash_typed<16>(ctx, g, gkind, out, in, out_parity, kappa, epi, e, x, dot);
-    }
+    if (out->prec == 64) return dslash_typed<64>(ctx, g, gkind, out, in, out_parity, kappa, epi, e, x, dot);
+    PkBatch B;
+    B.n          = 1;
+    B.out[0]     = out;
+    B.in[0]      = in;
+    B.x[0]       = x;
+    B.y[0]       = dot.y;
+    B.out_parity = out_parity;
+    B.kappa      = kappa;
+    B.epi        = epi;
+    B.e          = e;
+    B.dot_mode   = dot.mode;
+    B.fin        = dot.fin;
+    return launch_pdslash(ctx, g, gkind, B);
 }
 
 template <int P>
@@ -820,9 +844,17 @@ C2Q_EXPORT int c2q_gauge_download(const c2q_gauge* g, double* aos)
 // ---------------------------------------------------------------- spinors
 C2Q_EXPORT int c2q_spinor_eo_create(c2q_ctx* ctx, const c2q_lattice* lat, c2q_spinor_eo** out)
 {
+    return c2q_spinor_eo_create_precision(ctx, lat, C2Q_PREC_FP64, out);
+}
+
+C2Q_EXPORT int c2q_spinor_eo_create_precision(c2q_ctx* ctx, const c2q_lattice* lat, int precision,
+                                              c2q_spinor_eo** out)
+{
     if (!ctx || !lat || !out) return C2Q_BAD_ARG;
+    if (precision != 64 && precision != 32 && precision != 16)
+        return fail(ctx, C2Q_BAD_ARG, "precision must be 64, 32 or 16");
     c2q_spinor_eo* f = new c2q_spinor_eo();
-    int rc           = field_alloc(ctx, *lat, 64, f);
+    int rc           = field_alloc(ctx, *lat, precision, f);
     if (rc) {
         delete f;
         return rc;
@@ -881,8 +913,17 @@ static int aos_transfer(c2q_spinor_eo* f, double* host_dst, const double* host_s
 C2Q_EXPORT int c2q_spinor_eo_upload(c2q_spinor_eo* f, const double* aos)
 {
     if (!f || !aos) return C2Q_BAD_ARG;
-    if (f->prec != 64) return fail(f->ctx, C2Q_BAD_ARG, "upload needs an FP64 field");
-    int rc = aos_transfer(f, nullptr, aos, 0, 0, nullptr);
+    int rc = 0;
+    if (f->prec == 64) {
+        rc = aos_transfer(f, nullptr, aos, 0, 0, nullptr);
+    } else {  // through an FP64 field, rounded on the device
+        c2q_spinor_eo t;
+        rc = field_alloc(f->ctx, f->lat, 64, &t);
+        if (rc) return rc;
+        rc = aos_transfer(&t, nullptr, aos, 0, 0, nullptr);
+        if (!rc) rc = launch_convert(f->ctx, f, &t);
+        field_free(&t);
+    }
     if (rc) return rc;
     C2Q_CUDA(f->ctx, cudaStreamSynchronize(f->ctx->stream));
     return C2Q_OK;
@@ -894,9 +935,36 @@ C2Q_EXPORT int c2q_spinor_eo_download(const c2q_spinor_eo* f, double* aos)
     c2q_spinor_eo* ff = const_cast<c2q_spinor_eo*>(f);
     int rc            = ensure_staging(ff->ctx, (size_t)f->geom.seo * 24 * sizeof(double));
     if (rc) return rc;
-    rc = aos_transfer(ff, aos, nullptr, 0, 0, nullptr);
+    if (f->prec == 64) {
+        rc = aos_transfer(ff, aos, nullptr, 0, 0, nullptr);
+    } else {
+        c2q_spinor_eo t;
+        rc = field_alloc(f->ctx, f->lat, 64, &t);
+        if (rc) return rc;
+        rc = launch_convert(f->ctx, &t, f);
+        if (!rc) rc = aos_transfer(&t, aos, nullptr, 0, 0, nullptr);
+        if (!rc) C2Q_CUDA(f->ctx, cudaStreamSynchronize(f->ctx->stream));
+        field_free(&t);
+    }
     if (rc) return rc;
     C2Q_CUDA(f->ctx, cudaStreamSynchronize(f->ctx->stream));
+    return C2Q_OK;
+}
+
+C2Q_EXPORT int c2q_spinor_eo_precision(const c2q_spinor_eo* f) { return f ? f->prec : C2Q_BAD_ARG; }
+
+C2Q_EXPORT int c2q_spinor_eo_convert(c2q_spinor_eo* out, const c2q_spinor_eo* in)
+{
+    if (!out || !in) return C2Q_BAD_ARG;
+    if (!same_lattice(out->lat, in->lat)) return fail(out->ctx, C2Q_BAD_ARG, "lattice mismatch");
+    if (out == in) return C2Q_OK;
+    return launch_convert(out->ctx, out, in);
+}
+
+C2Q_EXPORT int c2q_ctx_set_link_format(c2q_ctx* ctx, int rec12)
+{
+    if (!ctx || (rec12 != 0 && rec12 != 1)) return C2Q_BAD_ARG;
+    ctx->rec12 = rec12;
     return C2Q_OK;
 }
 
@@ -944,7 +1012,7 @@ C2Q_EXPORT int c2q_convert_to_eoprec(c2q_spinor_eo* even, c2q_spinor_eo* odd, co
 
 C2Q_EXPORT int c2q_convert_from_eoprec(double* full, const c2q_spinor_eo* even, const c2q_spinor_eo* odd)
 {
-    if (!even || !odd || !full) return C2Q_BAD_ARG;
+    if (!even || !odd || !full || even->prec != 64 || odd->prec != 64) return C2Q_BAD_ARG;
     c2q_ctx* ctx       = even->ctx;
     const size_t bytes = (size_t)even->geom.seo * 2 * 24 * sizeof(double);
     int rc             = ensure_staging(ctx, bytes);
@@ -975,7 +1043,8 @@ C2Q_EXPORT int c2q_dslash_eo(c2q_spinor_eo* out, const c2q_gauge* g, const c2q_s
 {
     if (!out || !g || !in) return C2Q_BAD_ARG;
     if (evenodd != C2Q_EVEN && evenodd != C2Q_ODD) return fail(out->ctx, C2Q_BAD_ARG, "evenodd must be EVEN or ODD");
-    return launch_dslash(out->ctx, g, G64, out, in, evenodd == C2Q_ODD ? 0 : 1, kappa, EPI_PLAIN,
+    return launch_dslash(out->ctx, g, gkind_for(out->prec, out->ctx->rec12), out, in, evenodd == C2Q_ODD ? 0 : 1,
+                         kappa, EPI_PLAIN,
                          EpiArgs{1, 0, 1, 0, 0}, nullptr, DotSpec{});
 }
 
@@ -985,7 +1054,8 @@ C2Q_EXPORT int c2q_dslash_AND_M_tm_inverse_sitediagonal_eo(c2q_spinor_eo* out, c
 {
     if (!out || !g || !in) return C2Q_BAD_ARG;
     if (evenodd != C2Q_EVEN && evenodd != C2Q_ODD) return fail(out->ctx, C2Q_BAD_ARG, "evenodd must be EVEN or ODD");
-    return launch_dslash(out->ctx, g, G64, out, in, evenodd == C2Q_ODD ? 0 : 1, kappa, EPI_DIAG,
+    return launch_dslash(out->ctx, g, gkind_for(out->prec, out->ctx->rec12), out, in, evenodd == C2Q_ODD ? 0 : 1,
+                         kappa, EPI_DIAG,
                          diag_epi(mubar, minus ? C2Q_DIAG_M_TM_INVERSE_MINUS : C2Q_DIAG_M_TM_INVERSE, 0), nullptr,
                          DotSpec{});
 }
@@ -1020,10 +1090,12 @@ C2Q_EXPORT int c2q_apply_eo(int op, c2q_spinor_eo* out, const c2q_gauge* g, cons
     if (!out || !g || !in) return C2Q_BAD_ARG;
     c2q_ctx* ctx = out->ctx;
     c2q_spinor_eo t1, t2;
-    int rc = field_alloc(ctx, out->lat, 64, &t1);
+    int rc = field_alloc(ctx, out->lat, out->prec, &t1);
     if (rc) return rc;
-    rc = field_alloc(ctx, out->lat, 64, &t2);
-    if (!rc) rc = apply_operator(ctx, op, out, g, G64, in, kappa, mubar, action, &t1, &t2, DotSpec{}, nullptr);
+    rc = field_alloc(ctx, out->lat, out->prec, &t2);
+    if (!rc)
+        rc = apply_operator(ctx, op, out, g, gkind_for(out->prec, ctx->rec12), in, kappa, mubar, action, &t1, &t2,
+                            DotSpec{}, nullptr);
     field_free(&t1);
     field_free(&t2);
     return rc;

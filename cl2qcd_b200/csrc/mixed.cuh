@@ -1,69 +1,121 @@
-// mixed.cuh -- vector updates of the mixed-precision CG, where the residual
-// and the solution increment (precision PA) and the search direction and
-// operator output (precision PB) are stored in different precisions.
+// mixed.cuh -- vector updates of the mixed-precision CG on the paired-site
+// slots of pack.cuh: the residual and the solution increment are FP32 fields,
+// the search direction and the operator output are FP16 or FP32 (PB).  One
+// thread per slot (two sites), packed FP32 arithmetic; a launch covers a batch
+// of right-hand sides (block b: right-hand side b % nrhs), each with its own
+// solver scalars and its own reduction.
 #pragma once
 
 #include "blas.cuh"
+#include "pack.cuh"
 
 namespace c2q {
 
-// x_s = x_s + alpha p ; r_s = r_s - alpha v ; |r_s|^2 -> FIN_CG_BETA
-template <int PA, int PB>
-struct MixUpdateArgs {
-    SpinorPtr<PA> x, r;
-    SpinorPtr<PB> p, v;
-    const SolverScalars* sc;
-    int n, stride;
+constexpr int MIX_THREADS = 128;
+
+struct MixFields {
+    void* x;            // FP32 solution increment
+    void* r;            // FP32 residual
+    void* p;            // PB search direction
+    float* p_norm;
+    const void* v;      // PB operator output A p
+    const float* v_norm;
+    SolverScalars* sc;
+};
+
+struct MixArgs {
+    MixFields f[PK_MAX_RHS];
+    int nrhs;
+    int H, ss;
     RedArgs red;
 };
 
-template <int PA, int PB>
-__global__ void __launch_bounds__(BLAS_THREADS) mix_update_kernel(const MixUpdateArgs<PA, PB> A)
+// values of a PB field as s = scale * q (FP16: exact integers q and the
+// per-site scale; FP32: the values and scale 1)
+template <int PB>
+__device__ __forceinline__ void mix_load(const void* d, const float* n, int ss, int j, C2 s[12], float2* scale)
 {
-    const int i  = blockIdx.x * blockDim.x + threadIdx.x;
-    double dv[2] = {0.0, 0.0};
-    if (i < A.n) {
-        const Cplx<float> al = cmk<float>((float)A.sc->alpha[0], (float)A.sc->alpha[1]);
-        Cplx<float> a[12], b[12];
-        SpinorIO<PA>::load(A.x, A.stride, i, a);
-        SpinorIO<PB>::load(A.p, A.stride, i, b);
-#pragma unroll
-        for (int k = 0; k < 12; ++k) a[k] = a[k] + cmul(b[k], al);
-        SpinorIO<PA>::store(A.x, A.stride, i, a);
-        SpinorIO<PA>::load(A.r, A.stride, i, a);
-        SpinorIO<PB>::load(A.v, A.stride, i, b);
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            a[k] = a[k] - cmul(b[k], al);
-            dv[0] += (double)a[k].re * a[k].re + (double)a[k].im * a[k].im;
-        }
-        SpinorIO<PA>::store(A.r, A.stride, i, a);
+    if constexpr (PB == 16) {
+        SlotF16::load_q(d, n, ss, j, s, scale);
+    } else {
+        SlotF32::load(d, ss, j, s);
+        *scale = bc2(1.0f);
     }
-    __shared__ double smem[64];
-    block_sum<2>(dv, smem);
-    finish_reduction<2>(dv, A.red, smem);
+}
+template <int PB>
+__device__ __forceinline__ void mix_store(void* d, float* n, int ss, int j, const C2 s[12])
+{
+    if constexpr (PB == 16)
+        SlotF16::store(d, n, ss, j, s);
+    else
+        SlotF32::store(d, ss, j, s);
 }
 
-// p = r_s + beta p
-template <int PA, int PB>
-struct MixPArgs {
-    SpinorPtr<PB> p;
-    SpinorPtr<PA> r;
-    const SolverScalars* sc;
-    int n, stride;
-};
-template <int PA, int PB>
-__global__ void __launch_bounds__(BLAS_THREADS) mix_p_kernel(const MixPArgs<PA, PB> A)
+// a += c b for a complex coefficient c (broadcast pairs cre, cim, -cim)
+__device__ __forceinline__ C2 caxpy2(C2 a, float2 cre, float2 cim, float2 ncim, C2 b)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.n) return;
-    const Cplx<float> be = cmk<float>((float)A.sc->beta[0], (float)A.sc->beta[1]);
-    Cplx<float> p[12], r[12];
-    SpinorIO<PB>::load(A.p, A.stride, i, p);
-    SpinorIO<PA>::load(A.r, A.stride, i, r);
+    return C2{fma2(b.re, cre, fma2(b.im, ncim, a.re)), fma2(b.im, cre, fma2(b.re, cim, a.im))};
+}
+
+// x += alpha p ; r -= alpha v ; |r|^2 -> FIN_CG_BETA of the right-hand side
+template <int PB>
+__global__ void __launch_bounds__(MIX_THREADS) mix_update_kernel(const MixArgs A)
+{
+    const int nrhs     = A.nrhs;
+    const int rhs      = nrhs == 1 ? 0 : (int)(blockIdx.x % (unsigned)nrhs);
+    const int blk      = nrhs == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nrhs);
+    const int j        = blk * MIX_THREADS + threadIdx.x;
+    const MixFields& F = A.f[rhs];
+    float2 n2          = bc2(0.f);
+    if (j < A.H) {
+        const float ar = (float)F.sc->alpha[0], ai = (float)F.sc->alpha[1];
+        C2 a[12], b[12];
+        float2 bs;
+        SlotF32::load(F.x, A.ss, j, a);
+        mix_load<PB>(F.p, F.p_norm, A.ss, j, b, &bs);
+        float2 cr = mul2(bc2(ar), bs), ci = mul2(bc2(ai), bs), nci = mul2(bc2(-ai), bs);
 #pragma unroll
-    for (int k = 0; k < 12; ++k) p[k] = r[k] + cmul(p[k], be);
-    SpinorIO<PB>::store(A.p, A.stride, i, p);
+        for (int c = 0; c < 12; ++c) a[c] = caxpy2(a[c], cr, ci, nci, b[c]);
+        SlotF32::store(F.x, A.ss, j, a);
+        SlotF32::load(F.r, A.ss, j, a);
+        mix_load<PB>(F.v, F.v_norm, A.ss, j, b, &bs);
+        cr  = mul2(bc2(-ar), bs);
+        ci  = mul2(bc2(-ai), bs);
+        nci = mul2(bc2(ai), bs);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            a[c] = caxpy2(a[c], cr, ci, nci, b[c]);
+            n2   = fma2(a[c].re, a[c].re, fma2(a[c].im, a[c].im, n2));
+        }
+        SlotF32::store(F.r, A.ss, j, a);
+    }
+    double dv[2] = {(double)n2.x + (double)n2.y, 0.0};
+    __shared__ double smem[64];
+    block_sum<2>(dv, smem);
+    RedArgs ra = A.red;
+    ra.sc      = F.sc;
+    finish_reduction<2>(dv, ra, smem, rhs, nrhs);
+}
+
+// p = r + beta p
+template <int PB>
+__global__ void __launch_bounds__(MIX_THREADS) mix_p_kernel(const MixArgs A)
+{
+    const int nrhs     = A.nrhs;
+    const int rhs      = nrhs == 1 ? 0 : (int)(blockIdx.x % (unsigned)nrhs);
+    const int blk      = nrhs == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nrhs);
+    const int j        = blk * MIX_THREADS + threadIdx.x;
+    const MixFields& F = A.f[rhs];
+    if (j >= A.H) return;
+    const float br = (float)F.sc->beta[0], bi = (float)F.sc->beta[1];
+    C2 p[12], r[12];
+    float2 ps;
+    mix_load<PB>(F.p, F.p_norm, A.ss, j, p, &ps);
+    SlotF32::load(F.r, A.ss, j, r);
+    const float2 cr = mul2(bc2(br), ps), ci = mul2(bc2(bi), ps), nci = mul2(bc2(-bi), ps);
+#pragma unroll
+    for (int c = 0; c < 12; ++c) p[c] = caxpy2(r[c], cr, ci, nci, p[c]);
+    mix_store<PB>(F.p, F.p_norm, A.ss, j, p);
 }
 
 // x64 = x64 + (double) x_s ; x_s = 0   (reliable update accumulation in FP64)

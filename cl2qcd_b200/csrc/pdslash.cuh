@@ -1,0 +1,529 @@
+// pdslash.cuh -- the eo hopping term with the fused tm epilogues for the
+// reduced-precision (FP32, FP16 fixed point) fields, on the paired-site slots
+// of pack.cuh, for a batch of right-hand sides that share one gauge field.
+//
+// One thread computes one slot (two output sites) of one right-hand side,
+// with packed FP32 arithmetic throughout: each float2 holds the same quantity
+// for the two sites, so every multiply-add, add and multiply of the stencil is
+// one f32x2 instruction for two sites.  The operator and its epilogues are the
+// ones of dslash.cuh (the reference's dslash_eo, ocl_kernel/fermionmatrix_eo.cl:30-253,
+// fused with M_tm_inverse_sitediagonal and the Aee/saxpy_AND_gamma5 tail).
+//
+// Batches: block b works on right-hand side b % nrhs and slot block b / nrhs,
+// so the blocks that read the same links run side by side and each link
+// crosses HBM once per batch; reductions are kept per right-hand side.
+//
+// FP16 arithmetic: the neighbour's biased words are projected without first
+// removing the bias (a - b of two biased values is exact; a + b subtracts the
+// doubled bias first), all values stay integers in units of the site's scale,
+// and the scale (norm / 32767) of the neighbour site and the link scale 1/32767
+// are applied as one factor per hop and one per launch.
+#pragma once
+
+#include <type_traits>
+
+#include "dslash.cuh"
+#include "pack.cuh"
+#include "reduce.cuh"
+
+namespace c2q {
+
+constexpr int PK_THREADS = 128;
+
+// Fields of one right-hand side of a batch.
+struct PkRhs {
+    void* out;
+    float* out_norm;
+    const void* in;
+    const float* in_norm;
+    const void* x;        // EPI_AXPY operand (same parity as out)
+    const float* x_norm;
+    const void* y;        // DOT_Y partner
+    const float* y_norm;
+    SolverScalars* sc;    // finisher target of this right-hand side
+    double* result;       // FIN_STORE_RESULT target (2 doubles)
+};
+
+struct PkGeom {
+    int ns, nsh, nt2;     // NS, NS/2, NT/2
+    int H;                // slots = Seo/2
+    int ss;               // lane stride in slots
+    int vs_h;             // NS^3/2 (slots per time slice)
+    FastDiv div_nsh, div_ns;
+};
+
+template <int P>
+struct PkParams {
+    PkRhs r[PK_MAX_RHS];
+    int nrhs;
+    const void* gauge;
+    PkGeom g;
+    HopCoef c;
+    EpiArgs e;
+    int out_parity;
+    RedArgs red;
+};
+
+// hop weight k (pairs) and its negations
+struct Kc {
+    float2 re, im, nre, nim;
+};
+
+// -------------------------------------------------------------- projection
+// h = a + c b, c in {1, -1, i, -i} = CK 0..3, from biased FP16 words
+template <int CK>
+__device__ __forceinline__ C2 proj_words(uint2 a, uint2 b)
+{
+    const float2 m1 = bc2(-1.0f), nb2 = bc2(-FIX_BIAS2);
+    const float2 ar = blo(a), ai = bhi(a);
+    if (CK == 0) return C2{add2(add2(ar, nb2), blo(b)), add2(add2(ai, nb2), bhi(b))};
+    if (CK == 1) return C2{fma2(blo(b), m1, ar), fma2(bhi(b), m1, ai)};
+    if (CK == 2) return C2{fma2(bhi(b), m1, ar), add2(add2(ai, nb2), blo(b))};
+    return C2{add2(add2(ar, nb2), bhi(b)), fma2(blo(b), m1, ai)};
+}
+// same from FP32 values
+template <int CK>
+__device__ __forceinline__ C2 proj_vals(C2 a, C2 b)
+{
+    const float2 m1 = bc2(-1.0f);
+    if (CK == 0) return C2{add2(a.re, b.re), add2(a.im, b.im)};
+    if (CK == 1) return C2{fma2(b.re, m1, a.re), fma2(b.im, m1, a.im)};
+    if (CK == 2) return C2{fma2(b.im, m1, a.re), add2(a.im, b.re)};
+    return C2{add2(a.re, b.im), fma2(b.re, m1, a.im)};
+}
+
+// acc += k * (u s) with u = conj(c) in {1, -1, i, -i} = CU 0..3
+template <int CU, bool KREAL>
+__device__ __forceinline__ void acc_add(C2& a, float2 sre, float2 sim, const Kc& k)
+{
+    if (KREAL) {
+        if (CU == 0) {
+            a.re = fma2(sre, k.re, a.re);
+            a.im = fma2(sim, k.re, a.im);
+        } else if (CU == 1) {
+            a.re = fma2(sre, k.nre, a.re);
+            a.im = fma2(sim, k.nre, a.im);
+        } else if (CU == 2) {  // i s = (-sim, sre)
+            a.re = fma2(sim, k.nre, a.re);
+            a.im = fma2(sre, k.re, a.im);
+        } else {  // -i s = (sim, -sre)
+            a.re = fma2(sim, k.re, a.re);
+            a.im = fma2(sre, k.nre, a.im);
+        }
+    } else {
+        if (CU == 0) {
+            a.re = fma2(sre, k.re, fma2(sim, k.nim, a.re));
+            a.im = fma2(sim, k.re, fma2(sre, k.im, a.im));
+        } else if (CU == 1) {
+            a.re = fma2(sre, k.nre, fma2(sim, k.im, a.re));
+            a.im = fma2(sim, k.nre, fma2(sre, k.nim, a.im));
+        } else if (CU == 2) {
+            a.re = fma2(sim, k.nre, fma2(sre, k.nim, a.re));
+            a.im = fma2(sre, k.re, fma2(sim, k.nim, a.im));
+        } else {
+            a.re = fma2(sim, k.re, fma2(sre, k.im, a.re));
+            a.im = fma2(sre, k.nre, fma2(sim, k.im, a.im));
+        }
+    }
+}
+
+// One half-spinor channel: s = U h (or U^dagger h), acc_A += k s, acc_PP += conj(c) k s.
+template <int A, int PP, int CK, bool DAG, bool KREAL>
+__device__ __forceinline__ void pk_channel(C2 acc[12], const C2 h[3], const C2 u[9], const Kc& k)
+{
+    const float2 m1 = bc2(-1.0f);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        float2 sre, sim;
+        if (!DAG) {  // s_r = sum_c U[r][c] h_c
+            float2 p = mul2(u[3 * r].re, h[0].re), q = mul2(u[3 * r].im, h[0].im);
+            p        = fma2(u[3 * r + 1].re, h[1].re, p);
+            q        = fma2(u[3 * r + 1].im, h[1].im, q);
+            p        = fma2(u[3 * r + 2].re, h[2].re, p);
+            q        = fma2(u[3 * r + 2].im, h[2].im, q);
+            sre      = fma2(q, m1, p);
+            sim      = mul2(u[3 * r].re, h[0].im);
+            sim      = fma2(u[3 * r].im, h[0].re, sim);
+            sim      = fma2(u[3 * r + 1].re, h[1].im, sim);
+            sim      = fma2(u[3 * r + 1].im, h[1].re, sim);
+            sim      = fma2(u[3 * r + 2].re, h[2].im, sim);
+            sim      = fma2(u[3 * r + 2].im, h[2].re, sim);
+        } else {  // s_r = sum_c conj(U[c][r]) h_c
+            sre      = mul2(u[r].re, h[0].re);
+            sre      = fma2(u[r].im, h[0].im, sre);
+            sre      = fma2(u[3 + r].re, h[1].re, sre);
+            sre      = fma2(u[3 + r].im, h[1].im, sre);
+            sre      = fma2(u[6 + r].re, h[2].re, sre);
+            sre      = fma2(u[6 + r].im, h[2].im, sre);
+            float2 p = mul2(u[r].re, h[0].im), q = mul2(u[r].im, h[0].re);
+            p        = fma2(u[3 + r].re, h[1].im, p);
+            q        = fma2(u[3 + r].im, h[1].re, q);
+            p        = fma2(u[6 + r].re, h[2].im, p);
+            q        = fma2(u[6 + r].im, h[2].re, q);
+            sim      = fma2(q, m1, p);
+        }
+        acc_add<0, KREAL>(acc[3 * A + r], sre, sim, k);
+        acc_add<ConjUnit<CK>::value, KREAL>(acc[3 * PP + r], sre, sim, k);
+    }
+}
+
+// ------------------------------------------------------------------ staging
+// Every thread streams the data of its next hops into its own slices of a
+// shared-memory ring with cp.async (16 bytes per copy), so two or three hops
+// of loads are in flight while it computes the current one, without holding
+// them in registers.  A stage holds, as 16-byte chunks, the neighbour spinor
+// (FP16: 6 chunks + one for the norm pair; FP32: 12) followed by its link
+// (FP16: 3 chunks; FP32: NL).  Chunk c of stage s of thread t sits at
+// ring[(s * CH + c) * PK_THREADS + t]: consecutive threads read consecutive
+// 16-byte words.  Only the thread that copied a chunk reads it, so
+// cp.async.wait_group alone orders the copies and the reads.
+template <int P, int NL>
+struct PkStage {
+    static constexpr int SPC      = P == 16 ? 7 : 12;
+    static constexpr int LKC      = P == 16 ? 3 : NL;
+    static constexpr int CH       = SPC + LKC;
+    static constexpr int STAGES   = P == 16 ? 3 : 2;
+    static constexpr size_t BYTES = (size_t)STAGES * CH * 16 * PK_THREADS;
+};
+
+__device__ __forceinline__ void cp16(uint4* smem, const void* g)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp8(uint4* smem, const void* g)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// spinor of `slot` of field (d, norm) -> chunks [0, SPC) of a stage
+template <int P>
+__device__ __forceinline__ void stage_spinor(uint4* st, const void* d, const float* norm, int ss, int slot)
+{
+    const uint4* p  = static_cast<const uint4*>(d) + slot;
+    constexpr int n = P == 16 ? 6 : 12;
+#pragma unroll
+    for (int c = 0; c < n; ++c) cp16(st + c * PK_THREADS, p + (size_t)c * ss);
+    if (P == 16) cp8(st + 6 * PK_THREADS, reinterpret_cast<const float2*>(norm) + slot);
+}
+// link of `slot` of a (parity, mu) group -> chunks [SPC, CH)
+template <int P, int NL>
+__device__ __forceinline__ void stage_link(uint4* st, const char* links, int ss, int slot)
+{
+    constexpr int SPC = PkStage<P, NL>::SPC, LKC = PkStage<P, NL>::LKC;
+    const uint4* p    = reinterpret_cast<const uint4*>(links) + slot;
+#pragma unroll
+    for (int c = 0; c < LKC; ++c) cp16(st + (SPC + c) * PK_THREADS, p + (size_t)c * ss);
+}
+
+__device__ __forceinline__ float4 as_f4(uint4 v)
+{
+    return make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
+}
+
+// decode a staged link (chunks at lk[c * PK_THREADS])
+template <int P, int NL, bool SWP>
+__device__ __forceinline__ void staged_link(const uint4* lk, C2 u[9])
+{
+    if constexpr (P == 16) {
+        const float2 nb = bc2(-FIX_BIAS);
+#pragma unroll
+        for (int L = 0; L < 3; ++L) {
+            const uint4 v  = lk[L * PK_THREADS];
+            const uint2 wa = SWP ? make_uint2(v.y, v.x) : make_uint2(v.x, v.y);
+            const uint2 wb = SWP ? make_uint2(v.w, v.z) : make_uint2(v.z, v.w);
+            u[2 * L]       = C2{add2(blo(wa), nb), add2(bhi(wa), nb)};
+            u[2 * L + 1]   = C2{add2(blo(wb), nb), add2(bhi(wb), nb)};
+        }
+        reconstruct_row2_pk(u, 1.0f / 32767.0f);
+    } else {
+#pragma unroll
+        for (int e = 0; e < NL; ++e) u[e] = c2_from(as_f4(lk[e * PK_THREADS]), SWP);
+        if (NL == 6) reconstruct_row2_pk(u, 1.0f);
+    }
+}
+// FP16 words and norm pair of a staged spinor
+template <bool SWP>
+__device__ __forceinline__ void staged_words(const uint4* st, uint2 w[12], float2* nrm)
+{
+#pragma unroll
+    for (int L = 0; L < 6; ++L) {
+        const uint4 v = st[L * PK_THREADS];
+        w[2 * L]      = SWP ? make_uint2(v.y, v.x) : make_uint2(v.x, v.y);
+        w[2 * L + 1]  = SWP ? make_uint2(v.w, v.z) : make_uint2(v.z, v.w);
+    }
+    const float2 n = *reinterpret_cast<const float2*>(st + 6 * PK_THREADS);
+    *nrm           = SWP ? swap2(n) : n;
+}
+// FP32 values of a staged spinor
+template <bool SWP>
+__device__ __forceinline__ void staged_vals(const uint4* st, C2 s[12])
+{
+#pragma unroll
+    for (int c = 0; c < 12; ++c) s[c] = c2_from(as_f4(st[c * PK_THREADS]), SWP);
+}
+// a staged (unswapped) operand as values sc * q: FP16 exact integers and the
+// per-site scale, FP32 values and scale 1
+template <int P>
+__device__ __forceinline__ void staged_operand(const uint4* st, C2 q[12], float2* sc)
+{
+    if constexpr (P == 16) {
+        uint2 w[12];
+        float2 n;
+        staged_words<false>(st, w, &n);
+        *sc             = mul2(n, bc2(1.0f / 32767.0f));
+        const float2 nb = bc2(-FIX_BIAS);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) q[c] = C2{add2(blo(w[c]), nb), add2(bhi(w[c]), nb)};
+    } else {
+        staged_vals<false>(st, q);
+        *sc = bc2(1.0f);
+    }
+}
+
+// One hop from a stage: the neighbour slot (and, for a backward hop, its
+// link) may hold the two sites swapped -- SWP, set for the time hops across
+// the fold.  A forward hop's link sits at the output slot and is never swapped.
+template <int P, int NL, int MU, bool BACK, bool SWP, bool KREAL>
+__device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, double phre, double phim)
+{
+    using T          = Proj<MU>;
+    constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
+    constexpr int c1 = BACK ? NegUnit<T::c1>::value : T::c1;
+    C2 u[9];
+    staged_link<P, NL, BACK && SWP>(st + PkStage<P, NL>::SPC * PK_THREADS, u);
+    Kc k;
+    C2 h[3];
+    if constexpr (P == 16) {
+        uint2 w[12];
+        float2 nrm;
+        staged_words<SWP>(st, w, &nrm);
+        k.re  = mul2(bc2((float)phre), nrm);
+        k.nre = mul2(bc2((float)-phre), nrm);
+        if (!KREAL) {
+            k.im  = mul2(bc2((float)phim), nrm);
+            k.nim = mul2(bc2((float)-phim), nrm);
+        }
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_words<c0>(w[col], w[3 * T::p0 + col]);
+        pk_channel<0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_words<c1>(w[3 + col], w[3 * T::p1 + col]);
+        pk_channel<1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
+    } else {
+        C2 psi[12];
+        staged_vals<SWP>(st, psi);
+        k.re  = bc2((float)phre);
+        k.nre = bc2((float)-phre);
+        k.im  = bc2((float)phim);
+        k.nim = bc2((float)-phim);
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_vals<c0>(psi[col], psi[3 * T::p0 + col]);
+        pk_channel<0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_vals<c1>(psi[3 + col], psi[3 * T::p1 + col]);
+        pk_channel<1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
+    }
+}
+
+// hop q = 2 mu + back, with the phase pattern resolved
+template <int P, int NL, int MU, bool BACK, bool SWP, int PH>
+__device__ __forceinline__ void pk_hop_ph(C2 acc[12], const PkParams<P>& prm, const uint4* st)
+{
+    const int d      = BACK ? 1 : 0;
+    const double pre = prm.c.re[MU][d], pim = prm.c.im[MU][d];
+    if (PH == PH_REAL || (PH == PH_TCPLX && MU != 0)) {
+        pk_hop<P, NL, MU, BACK, SWP, true>(acc, st, pre, pim);
+    } else if (PH == PH_TCPLX) {
+        pk_hop<P, NL, MU, BACK, SWP, false>(acc, st, pre, pim);
+    } else if ((prm.c.real_mask >> (2 * MU + d)) & 1u) {
+        pk_hop<P, NL, MU, BACK, SWP, true>(acc, st, pre, pim);
+    } else {
+        pk_hop<P, NL, MU, BACK, SWP, false>(acc, st, pre, pim);
+    }
+}
+
+// 16-byte lanes per (parity, mu) group of links in the slot layout
+template <int P, int NL>
+__host__ __device__ constexpr int pk_link_lanes()
+{
+    return P == 16 ? 3 : NL;
+}
+
+template <int P, int NL, int EPI, int DOT, int PH>
+__global__ void __launch_bounds__(PK_THREADS, P == 16 ? 3 : 2) pdslash_kernel(const PkParams<P> prm)
+{
+    using S = PkStage<P, NL>;
+    static_assert(S::STAGES == 2 || S::STAGES == 3, "the prologue below issues one or two stages");
+    extern __shared__ uint4 ring[];
+    uint4* mine     = ring + threadIdx.x;
+    const PkGeom& g = prm.g;
+    const int nrhs  = prm.nrhs;
+    const int rhs   = nrhs == 1 ? 0 : (int)(blockIdx.x % (unsigned)nrhs);
+    const int blk   = nrhs == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nrhs);
+    const int j     = blk * PK_THREADS + threadIdx.x;
+    const PkRhs& rr = prm.r[rhs];
+    float2 dre = bc2(0.f), dim = bc2(0.f), dq = bc2(0.f);
+
+    if (j < g.H) {
+        // coordinates of slot j (site 0 at time t < NT/2; site 1 at t + NT/2)
+        const unsigned r1 = fdiv((unsigned)j, g.div_nsh);
+        const int xh      = j - (int)r1 * g.nsh;
+        const unsigned r2 = fdiv(r1, g.div_ns);
+        const int y       = (int)r1 - (int)r2 * g.ns;
+        const int t       = (int)fdiv(r2, g.div_ns);
+        const int z       = (int)r2 - t * g.ns;
+        const int x       = 2 * xh + ((prm.out_parity + y + z + t) & 1);
+        const int yzt     = j - xh;
+        const int ss      = g.ss;
+
+        const int po          = prm.out_parity;
+        constexpr int LL      = pk_link_lanes<P, NL>();
+        const size_t grp      = (size_t)LL * ss * 16;
+        const char* gb        = static_cast<const char*>(prm.gauge);
+        const char* fwd_links = gb + (size_t)(po * 4) * grp;
+        const char* bwd_links = gb + (size_t)((1 - po) * 4) * grp;
+
+        // neighbour slot and link slot of the 8 hops (q = 2 mu + back); across
+        // the fold in time the neighbour slot holds the pair swapped
+        const bool fold_f = t + 1 == g.nt2, fold_b = t == 0;
+        const int base    = j - g.vs_h * t;
+        int nb[8];
+        nb[0]        = fold_f ? base : j + g.vs_h;
+        nb[1]        = fold_b ? base + g.vs_h * (g.nt2 - 1) : j - g.vs_h;
+        const int xp = x + 1 == g.ns ? 0 : x + 1, xm = x == 0 ? g.ns - 1 : x - 1;
+        nb[2]        = (xp >> 1) + yzt;
+        nb[3]        = (xm >> 1) + yzt;
+        const int row = g.nsh, pl = g.nsh * g.ns;
+        nb[4]         = y + 1 == g.ns ? j - (g.ns - 1) * row : j + row;
+        nb[5]         = y == 0 ? j + (g.ns - 1) * row : j - row;
+        nb[6]         = z + 1 == g.ns ? j - (g.ns - 1) * pl : j + pl;
+        nb[7]         = z == 0 ? j + (g.ns - 1) * pl : j - pl;
+
+        // stage q: hops 0..7, then the epilogue operands x (q = 8) and y (q = 9);
+        // every index below is a compile-time constant
+        auto issue = [&](auto qc) {
+            constexpr int q = decltype(qc)::value;
+            uint4* st       = mine + (size_t)((q % S::STAGES) * S::CH) * PK_THREADS;
+            if constexpr (q < 8) {
+                constexpr bool back = q & 1;
+                stage_spinor<P>(st, rr.in, rr.in_norm, ss, nb[q]);
+                stage_link<P, NL>(st, (back ? bwd_links : fwd_links) + (size_t)(q >> 1) * grp, ss, back ? nb[q] : j);
+            } else if constexpr (q == 8) {
+                if (EPI == EPI_AXPY) stage_spinor<P>(st, rr.x, rr.x_norm, ss, j);
+            } else {
+                if (DOT == DOT_Y) stage_spinor<P>(st, rr.y, rr.y_norm, ss, j);
+            }
+            cp_commit();
+        };
+
+        C2 acc[12];
+#pragma unroll
+        for (int c = 0; c < 12; ++c) acc[c] = C2{bc2(0.f), bc2(0.f)};
+
+        auto step = [&](auto hc) {
+            constexpr int h = decltype(hc)::value;
+            if constexpr (h + S::STAGES - 1 <= 9)
+                issue(std::integral_constant<int, h + S::STAGES - 1>{});
+            else
+                cp_commit();
+            cp_wait<S::STAGES - 1>();
+            const uint4* st = mine + (size_t)((h % S::STAGES) * S::CH) * PK_THREADS;
+            constexpr int mu = h >> 1;
+            constexpr bool back = h & 1;
+            if constexpr (mu == 0) {
+                if (back ? fold_b : fold_f)
+                    pk_hop_ph<P, NL, 0, back, true, PH>(acc, prm, st);
+                else
+                    pk_hop_ph<P, NL, 0, back, false, PH>(acc, prm, st);
+            } else {
+                pk_hop_ph<P, NL, mu, back, false, PH>(acc, prm, st);
+            }
+        };
+        issue(std::integral_constant<int, 0>{});
+        if constexpr (S::STAGES > 2) issue(std::integral_constant<int, 1>{});
+        step(std::integral_constant<int, 0>{});
+        step(std::integral_constant<int, 1>{});
+        step(std::integral_constant<int, 2>{});
+        step(std::integral_constant<int, 3>{});
+        step(std::integral_constant<int, 4>{});
+        step(std::integral_constant<int, 5>{});
+        step(std::integral_constant<int, 6>{});
+        step(std::integral_constant<int, 7>{});
+        if constexpr (S::STAGES == 2) issue(std::integral_constant<int, 9>{});
+        cp_wait<0>();
+
+        // epilogue on h = scale * acc (scale = -kappa, times the FP16 scales)
+        const float sc = (float)prm.c.scale;
+        if (EPI == EPI_PLAIN) {
+#pragma unroll
+            for (int c = 0; c < 12; ++c) acc[c] = C2{mul2(acc[c].re, bc2(sc)), mul2(acc[c].im, bc2(sc))};
+        } else if (EPI == EPI_DIAG) {
+#pragma unroll
+            for (int c = 0; c < 12; ++c) {
+                const float fr = (float)(c < 6 ? prm.e.f1re : prm.e.f2re) * sc;
+                const float fi = (float)(c < 6 ? prm.e.f1im : prm.e.f2im) * sc;
+                const C2 a     = acc[c];
+                acc[c]         = C2{fma2(a.re, bc2(fr), mul2(a.im, bc2(-fi))), fma2(a.im, bc2(fr), mul2(a.re, bc2(fi)))};
+            }
+        } else if (EPI == EPI_AXPY) {
+            // [g5] (f x - sc acc); FP16 x as exact integers q with the per-site
+            // scale folded into f, the sign of g5 folded into the coefficients
+            C2 xv[12];
+            float2 xs;
+            staged_operand<P>(mine + (size_t)((8 % S::STAGES) * S::CH) * PK_THREADS, xv, &xs);
+#pragma unroll
+            for (int c = 0; c < 12; ++c) {
+                const float gs  = (prm.e.gamma5 && c >= 6) ? -1.0f : 1.0f;
+                const float2 fr = mul2(bc2(gs * (float)(c < 6 ? prm.e.f1re : prm.e.f2re)), xs);
+                const float2 fi = mul2(bc2(gs * (float)(c < 6 ? prm.e.f1im : prm.e.f2im)), xs);
+                const float2 nf = mul2(bc2(-gs * (float)(c < 6 ? prm.e.f1im : prm.e.f2im)), xs);
+                const float ms  = -gs * sc;
+                const C2 a      = acc[c];
+                acc[c]          = C2{fma2(a.re, bc2(ms), fma2(xv[c].re, fr, mul2(xv[c].im, nf))),
+                            fma2(a.im, bc2(ms), fma2(xv[c].im, fr, mul2(xv[c].re, fi)))};
+            }
+        }
+        if constexpr (P == 16)
+            SlotF16::store(rr.out, rr.out_norm, ss, j, acc);
+        else
+            SlotF32::store(rr.out, ss, j, acc);
+
+        if (DOT == DOT_Y) {  // conj(y) out, FP16 y as integers times the per-site scale
+            C2 yv[12];
+            float2 ys;
+            staged_operand<P>(mine + (size_t)((9 % S::STAGES) * S::CH) * PK_THREADS, yv, &ys);
+#pragma unroll
+            for (int c = 0; c < 12; ++c) {
+                dre = fma2(yv[c].re, acc[c].re, fma2(yv[c].im, acc[c].im, dre));
+                dim = fma2(yv[c].re, acc[c].im, dim);
+                dq  = fma2(yv[c].im, acc[c].re, dq);
+            }
+            dre = mul2(dre, ys);
+            dim = mul2(dim, ys);
+            dq  = mul2(dq, ys);
+        } else if (DOT == DOT_SELF) {
+#pragma unroll
+            for (int c = 0; c < 12; ++c) dre = fma2(acc[c].re, acc[c].re, fma2(acc[c].im, acc[c].im, dre));
+        }
+    }
+    if (DOT != DOT_NONE) {
+        double dv[2] = {(double)dre.x + (double)dre.y,
+                        ((double)dim.x - (double)dq.x) + ((double)dim.y - (double)dq.y)};
+        __shared__ double smem[2 * 32];
+        block_sum<2>(dv, smem);
+        RedArgs ra = prm.red;
+        if (rr.sc) ra.sc = rr.sc;
+        if (rr.result) ra.result = rr.result;
+        finish_reduction<2>(dv, ra, smem, rhs, nrhs);
+    }
+}
+
+}  // namespace c2q

@@ -81,32 +81,37 @@ __device__ __forceinline__ void cdiv_store(double* out, const double* n, const d
 }
 
 // Called by every thread of every block after block_sum (value in thread 0).
+// Batched launches reduce per group: block b belongs to group b % G (one
+// group per right-hand side), each group has its own ticket ra.ticket[grp]
+// and its last block sums that group's partials in block order.
 template <int NV>
-__device__ __forceinline__ void finish_reduction(const double v[NV], const RedArgs& ra, double* smem)
+__device__ __forceinline__ void finish_reduction(const double v[NV], const RedArgs& ra, double* smem, int grp = 0,
+                                                 int G = 1)
 {
     __shared__ bool last;
+    const int nb = (int)gridDim.x / G;  // blocks of this group
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int k = 0; k < NV; ++k) ra.partials[(size_t)blockIdx.x * NV + k] = v[k];
         __threadfence();
-        const unsigned t = atomicAdd(ra.ticket, 1u);
-        last             = (t == gridDim.x - 1);
+        const unsigned t = atomicAdd(ra.ticket + grp, 1u);
+        last             = (t == (unsigned)nb - 1u);
     }
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // fixed-order sum of the partials: thread j takes a contiguous chunk
+    // fixed-order sum of the group's partials: thread j takes a contiguous chunk
     double acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-    const int n = gridDim.x, chunk = (n + blockDim.x - 1) / blockDim.x;
-    const int lo = threadIdx.x * chunk, hi = min(n, lo + chunk);
-    for (int b = lo; b < hi; ++b)
+    const int chunk = (nb + blockDim.x - 1) / blockDim.x;
+    const int lo = threadIdx.x * chunk, hi = min(nb, lo + chunk);
+    for (int m = lo; m < hi; ++m)
 #pragma unroll
-        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(ra.partials + (size_t)b * NV + k);
+        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(ra.partials + ((size_t)m * G + grp) * NV + k);
     block_sum<NV>(acc, smem);
     if (threadIdx.x == 0) {
-        *ra.ticket = 0u;
+        ra.ticket[grp] = 0u;
         SolverScalars* s = ra.sc;
         switch (ra.fin) {
             case FIN_STORE_RESULT:

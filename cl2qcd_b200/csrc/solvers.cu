@@ -118,12 +118,6 @@ int copy_field(c2q_ctx* ctx, c2q_spinor_eo* to, const c2q_spinor_eo* from)
     return launch_blas(ctx, s);
 }
 
-int gkind_for(int prec, int rec12)
-{
-    if (prec == 64) return rec12 ? G64R12 : G64;
-    if (prec == 32) return rec12 ? G32R12 : G32;
-    return G16R12;
-}
 
 // ||b - A x||^2 in FP64 (true residual); r receives b - A x.
 int true_residual(c2q_ctx* ctx, int op, const c2q_gauge* g, const c2q_spinor_eo* x, const c2q_spinor_eo* b,
@@ -351,18 +345,42 @@ int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2
 // residual has dropped by `reliable_delta` since the last update (or reached
 // the stopping threshold), the increment is added to the FP64 solution and the
 // residual is recomputed from scratch in FP64 with FP64 links.
-template <int PB>
-int mix_update(c2q_ctx* ctx, c2q_spinor_eo* xs, c2q_spinor_eo* rs, const c2q_spinor_eo* p, const c2q_spinor_eo* v)
+// Batched mixed-precision vector updates: entry r of each array is one
+// right-hand side (FP32 xs, rs; PB p, v; its solver scalars).
+struct MixBatch {
+    int n = 0;
+    c2q_spinor_eo* xs[MAX_BATCH] = {};
+    c2q_spinor_eo* rs[MAX_BATCH] = {};
+    c2q_spinor_eo* p[MAX_BATCH]  = {};
+    const c2q_spinor_eo* v[MAX_BATCH] = {};
+    SolverScalars* sc[MAX_BATCH] = {};
+};
+
+static MixArgs mix_args(const MixBatch& B)
 {
-    MixUpdateArgs<32, PB> A;
-    A.x      = sptr<32>(xs);
-    A.r      = sptr<32>(rs);
-    A.p      = sptr<PB>(p);
-    A.v      = sptr<PB>(v);
-    A.sc     = ctx->scalars;
-    A.n      = xs->geom.seo;
-    A.stride = xs->geom.stride;
-    const int blocks = (A.n + BLAS_THREADS - 1) / BLAS_THREADS;
+    MixArgs A;
+    memset(&A, 0, sizeof A);
+    for (int r = 0; r < B.n; ++r) {
+        MixFields& F = A.f[r];
+        F.x          = B.xs[r] ? B.xs[r]->data : nullptr;
+        F.r          = B.rs[r]->data;
+        F.p          = B.p[r]->data;
+        F.p_norm     = B.p[r]->norm;
+        F.v          = B.v[r] ? B.v[r]->data : nullptr;
+        F.v_norm     = B.v[r] ? B.v[r]->norm : nullptr;
+        F.sc         = B.sc[r];
+    }
+    A.nrhs = B.n;
+    A.H    = B.rs[0]->geom.seo / 2;
+    A.ss   = B.rs[0]->geom.stride / 2;
+    return A;
+}
+
+template <int PB>
+int mix_update_batch(c2q_ctx* ctx, const MixBatch& B)
+{
+    MixArgs A        = mix_args(B);
+    const int blocks = (A.H + MIX_THREADS - 1) / MIX_THREADS * B.n;
     int rc           = ensure_partials(ctx, blocks);
     if (rc) return rc;
     A.red.partials = ctx->partials;
@@ -370,25 +388,45 @@ int mix_update(c2q_ctx* ctx, c2q_spinor_eo* xs, c2q_spinor_eo* rs, const c2q_spi
     A.red.result   = ctx->red_result;
     A.red.sc       = ctx->scalars;
     A.red.fin      = FIN_CG_BETA;
-    mix_update_kernel<32, PB><<<blocks, BLAS_THREADS, 0, ctx->stream>>>(A);
+    mix_update_kernel<PB><<<blocks, MIX_THREADS, 0, ctx->stream>>>(A);
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
 }
 
 template <int PB>
-int mix_p(c2q_ctx* ctx, c2q_spinor_eo* p, const c2q_spinor_eo* rs)
+int mix_p_batch(c2q_ctx* ctx, const MixBatch& B)
 {
-    MixPArgs<32, PB> A;
-    A.p      = sptr<PB>(p);
-    A.r      = sptr<32>(rs);
-    A.sc     = ctx->scalars;
-    A.n      = p->geom.seo;
-    A.stride = p->geom.stride;
-    mix_p_kernel<32, PB><<<(A.n + BLAS_THREADS - 1) / BLAS_THREADS, BLAS_THREADS, 0, ctx->stream>>>(A);
+    const MixArgs A  = mix_args(B);
+    const int blocks = (A.H + MIX_THREADS - 1) / MIX_THREADS * B.n;
+    mix_p_kernel<PB><<<blocks, MIX_THREADS, 0, ctx->stream>>>(A);
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
+}
+
+template <int PB>
+int mix_update(c2q_ctx* ctx, c2q_spinor_eo* xs, c2q_spinor_eo* rs, c2q_spinor_eo* p, const c2q_spinor_eo* v)
+{
+    MixBatch B;
+    B.n     = 1;
+    B.xs[0] = xs;
+    B.rs[0] = rs;
+    B.p[0]  = p;
+    B.v[0]  = v;
+    B.sc[0] = ctx->scalars;
+    return mix_update_batch<PB>(ctx, B);
+}
+
+template <int PB>
+int mix_p(c2q_ctx* ctx, c2q_spinor_eo* p, c2q_spinor_eo* rs)
+{
+    MixBatch B;
+    B.n     = 1;
+    B.rs[0] = rs;
+    B.p[0]  = p;
+    B.sc[0] = ctx->scalars;
+    return mix_p_batch<PB>(ctx, B);
 }
 
 int accumulate(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* xs)

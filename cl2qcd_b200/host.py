@@ -85,6 +85,10 @@ class System:
     def launch_count(self) -> int:
         return self.lib.c2q_ctx_launch_count(self.h)
 
+    def set_link_format(self, rec12: bool):
+        """Links read by the explicit operator calls: 18-real (default) or 12-real."""
+        _check(self.lib.c2q_ctx_set_link_format(self.h, int(bool(rec12))), self.h, self.lib)
+
     def close(self):
         if getattr(self, "h", None):
             for child in list(self._children):
@@ -175,12 +179,16 @@ class Gaugefield:
 
 
 class Spinorfield_eo:
-    def __init__(self, system: System, lattice: Lattice, aos: np.ndarray | None = None):
+    """An eo spinor field.  `precision` 64 is the reference's; 32 / 16 are the
+    reduced-precision storages of the mixed solvers (NT a multiple of 4)."""
+
+    def __init__(self, system: System, lattice: Lattice, aos: np.ndarray | None = None, precision: int = 64):
         self.system, self.lattice = system, lattice
+        self.precision = precision
         lib = system.lib
         h = C.c_void_p()
         lc = lattice.c()
-        _check(lib.c2q_spinor_eo_create(system.h, C.byref(lc), C.byref(h)), system.h, lib)
+        _check(lib.c2q_spinor_eo_create_precision(system.h, C.byref(lc), precision, C.byref(h)), system.h, lib)
         self.h = h
         system._adopt(self)
         if aos is not None:
@@ -205,6 +213,10 @@ class Spinorfield_eo:
 
     def gamma5(self):
         _check(self.system.lib.c2q_gamma5_eo(self.h), self.system.h, self.system.lib)
+
+    def convert_from(self, other: "Spinorfield_eo"):
+        """self = other rounded (or widened) to this field's precision."""
+        _check(self.system.lib.c2q_spinor_eo_convert(self.h, other.h), self.system.h, self.system.lib)
 
     def _destroy(self):
         if getattr(self, "h", None) and getattr(self.system, "h", None):

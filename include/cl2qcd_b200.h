@@ -167,7 +167,7 @@ C2Q_EXPORT int c2q_gauge_destroy(c2q_gauge* g);
 /* Device bytes held by the gauge object (all precisions built so far). */
 C2Q_EXPORT size_t c2q_gauge_device_bytes(const c2q_gauge* g);
 
-/* ---------------- eo spinor fields (FP64) ---------------- */
+/* ---------------- eo spinor fields ---------------- */
 /* physics::lattices::Spinorfield_eo (physics/lattices/spinorfield_eo.hpp:48-305). */
 C2Q_EXPORT int c2q_spinor_eo_create(c2q_ctx* ctx, const c2q_lattice* lat, c2q_spinor_eo** out);
 C2Q_EXPORT int c2q_spinor_eo_destroy(c2q_spinor_eo* f);
@@ -177,8 +177,23 @@ C2Q_EXPORT int c2q_spinor_eo_download(const c2q_spinor_eo* f, double* aos);
 /* Spinorfield_eo::zero / cold (physics/lattices/spinorfield_eo.cpp:147-165) */
 C2Q_EXPORT int c2q_spinor_eo_zero(c2q_spinor_eo* f);
 C2Q_EXPORT int c2q_spinor_eo_cold(c2q_spinor_eo* f);
+/* Reduced-precision eo fields (no counterpart in the reference, which is FP64
+ * only; CMakeLists.txt:127-132): C2Q_PREC_FP32 or C2Q_PREC_FP16 storage, the
+ * inner fields of the mixed-precision solvers.  NT must be a multiple of 4
+ * (the device layout pairs the sites at t and t + NT/2).  upload / download /
+ * zero / BLAS / the explicit operators accept them; upload rounds on the device.
+ * Fields passed together to one call must have the same precision. */
+C2Q_EXPORT int c2q_spinor_eo_create_precision(c2q_ctx* ctx, const c2q_lattice* lat, int precision,
+                                              c2q_spinor_eo** out);
+C2Q_EXPORT int c2q_spinor_eo_precision(const c2q_spinor_eo* f);
+/* out = in, rounded (or widened) to out's precision. */
+C2Q_EXPORT int c2q_spinor_eo_convert(c2q_spinor_eo* out, const c2q_spinor_eo* in);
+/* Link storage the explicit operator calls (dslash, dslash_AND_M_tm_inverse_sitediagonal,
+ * apply_eo) read: 0 = 18-real (the reference's), 1 = 12-real with row-2
+ * reconstruction.  FP16 operators always use 12-real FP16 links. */
+C2Q_EXPORT int c2q_ctx_set_link_format(c2q_ctx* ctx, int rec12);
 /* convert_to_eoprec / convert_from_eoprec (physics/lattices/spinorfield_eo.cpp:372-410):
- * `full` is a host spinor[V]; `even` gets the sites with x+y+z+t even. */
+ * `full` is a host spinor[V]; `even` gets the sites with x+y+z+t even (FP64 fields). */
 C2Q_EXPORT int c2q_convert_to_eoprec(c2q_spinor_eo* even, c2q_spinor_eo* odd, const double* full);
 C2Q_EXPORT int c2q_convert_from_eoprec(double* full, const c2q_spinor_eo* even, const c2q_spinor_eo* odd);
 

@@ -83,3 +83,44 @@ def test_rec12_matches_18real(port, system, O, lat):
                                                      use_rec12=True), add, r2)
     assert r2["true_resid_rel"] <= 1e-11
     assert rel_l2(x12.dump(), x64.dump()) < 1e-9
+
+
+RP_LATTICES = [(4, 4, 0.0, 0.0, None, None), (8, 8, 1.0, 0.0, None, None), (6, 8, 1.0, 0.3, None, None),
+               (8, 4, 0.7, 0.2, 0.1, 0.2), (4, 12, 1.0, 0.0, None, 0.3)]
+
+
+@pytest.mark.parametrize("lat", RP_LATTICES)
+@pytest.mark.parametrize("precision,rec12", [(32, False), (32, True), (16, True)])
+def test_reduced_precision_operators_match_oracle(port, system, O, lat, precision, rec12):
+    """The FP32 / FP16 paired-site sweeps against the FP64 oracle: the dslash on
+    both parities, the fused dslash + M_tm^{-1}, and Q+Q- (all four fused sweep
+    kinds).  Bound: a few units of the storage rounding (FP32 2^-24, FP16 fixed
+    point 2^-15 relative to the site norm) amplified by the stencil."""
+    import cl2qcd_b200 as c2q
+    tol = {32: 2e-6, 16: 2e-4}[precision]
+    L, g, gf = setup(port, c2q, system, lat)
+    system.set_link_format(rec12)
+    try:
+        s = port.pseudo_randomize(port.seo, 7)
+        a = c2q.Spinorfield_eo(system, L, s, precision=precision)
+        b = c2q.Spinorfield_eo(system, L, precision=precision)
+        for evenodd in (0, 1):
+            ref = port.dslash_eo(s, g, evenodd, 0.1573)
+            c2q.host.dslash(b, gf, a, evenodd, 0.1573)
+            assert rel_l2(b.dump(), ref) <= tol, ("dslash", evenodd)
+            ref = port.dslash_tm_inv_eo(s, g, evenodd, 0.16, 0.0016, False)
+            c2q.host.dslash_AND_M_tm_inverse_sitediagonal(b, gf, a, evenodd, 0.16, 0.0016, False)
+            assert rel_l2(b.dump(), ref) <= tol, ("dslash_tm_inv", evenodd)
+        ref = port.apply(O.OP_QPQM_EO, s, g, 0.16, 0.0016)
+        c2q.host.QplusQminus_eo()(b, gf, a, c2q.AdditionalParameters(0.16, 0.0016))
+        assert rel_l2(b.dump(), ref) <= 4 * tol, "QplusQminus_eo"
+        # round trip of the storage itself
+        assert rel_l2(a.dump(), s) <= tol / 4
+    finally:
+        system.set_link_format(False)
+
+
+def test_reduced_precision_needs_nt_multiple_of_4(system):
+    import cl2qcd_b200 as c2q
+    with pytest.raises(c2q.InvalidParameters):
+        c2q.Spinorfield_eo(system, c2q.Lattice(4, 6), precision=16)
