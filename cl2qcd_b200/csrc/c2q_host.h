@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <string>
 #include <vector>
 
@@ -56,6 +57,14 @@ struct c2q_ctx {
     std::vector<cudaEvent_t> event_pool;
     // link storage of the explicit operator entry points: 0 18-real, 1 12-real
     int rec12 = 0;
+    // autotuner of the paired-site dslash: launch shape -> chosen configuration
+    struct TuneEntry {
+        int cfg;
+        float us[4];
+    };
+    std::map<std::vector<int>, TuneEntry> tune;
+    c2q::SolverScalars* tune_scratch = nullptr;  // reductions of tuning launches land here
+    bool autotune = true;
 };
 
 struct c2q_gauge {

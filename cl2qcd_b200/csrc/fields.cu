@@ -650,6 +650,7 @@ C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream)
     if (device < 0 || device >= n) return C2Q_BAD_ARG;
     c2q_ctx* ctx = new c2q_ctx();
     ctx->device  = device;
+    if (const char* at = getenv("C2Q_AUTOTUNE")) ctx->autotune = at[0] != '0';
     int rc       = C2Q_OK;
     auto chk     = [&](cudaError_t e, const char* w) {
         if (e != cudaSuccess && rc == C2Q_OK) rc = cuda_fail(ctx, e, w);
@@ -695,6 +696,7 @@ C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->partials);
     cudaFree(ctx->ticket);
+    if (ctx->tune_scratch) cudaFree(ctx->tune_scratch);
     cudaFree(ctx->red_result);
     cudaFree(ctx->scalars);
     cudaFree(ctx->staging);

@@ -1,13 +1,91 @@
 // pdslash.cu -- host side of the paired-site dslash (pdslash.cuh): launches
 // for one right-hand side (the FP32 / FP16 branch of launch_dslash) and for
 // batches of right-hand sides sharing one gauge field.
+#include <cstdio>
+#include <cstring>
+
 #include "c2q_host.h"
 #include "pdslash.cuh"
 
 namespace c2q {
 
-void pk_dispatch32(const PkParams<32>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
-void pk_dispatch16(const PkParams<16>& prm, int epi, int dot, int blocks, cudaStream_t s);
+void pk_dispatch32_c0(const PkParams<32>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
+void pk_dispatch32_c1(const PkParams<32>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
+void pk_dispatch16_c0(const PkParams<16>& prm, int epi, int dot, int blocks, cudaStream_t s);
+void pk_dispatch16_c1(const PkParams<16>& prm, int epi, int dot, int blocks, cudaStream_t s);
+
+template <int P>
+static void pk_dispatch(const PkParams<P>& prm, int cfg, int nl, int epi, int dot, int blocks, cudaStream_t s)
+{
+    if constexpr (P == 16) {
+        if (cfg)
+            pk_dispatch16_c1(prm, epi, dot, blocks, s);
+        else
+            pk_dispatch16_c0(prm, epi, dot, blocks, s);
+    } else {
+        if (cfg)
+            pk_dispatch32_c1(prm, nl, epi, dot, blocks, s);
+        else
+            pk_dispatch32_c0(prm, nl, epi, dot, blocks, s);
+    }
+}
+
+// Autotuner: the first launch of each shape (precision, link format,
+// epilogue, reduction, phase pattern, batch size, volume) outside stream
+// capture times every configuration -- one warm-up launch, then two timed
+// launches each, with the reductions redirected to scratch so the caller's
+// solver scalars are untouched -- and keeps the fastest.  The launches are
+// idempotent (the output depends only on the inputs), so tuning does not
+// change results.  Shapes first met inside a graph capture use
+// configuration 0 and are not recorded.
+template <int P>
+static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int dot, int blocks, int* cfg)
+{
+    *cfg = 0;
+    if (!ctx->autotune) return C2Q_OK;
+    const unsigned m = prm.c.real_mask;
+    const int ph     = m == 0xFFu ? 0 : ((m & 0xFCu) == 0xFCu ? 1 : 2);
+    std::vector<int> key{P, nl, epi, dot, ph, prm.nrhs, 2 * prm.g.H};
+    auto it = ctx->tune.find(key);
+    if (it != ctx->tune.end()) {
+        *cfg = it->second.cfg;
+        return C2Q_OK;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    C2Q_CUDA(ctx, cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return C2Q_OK;
+    if (!ctx->tune_scratch)
+        C2Q_CUDA(ctx, cudaMalloc(&ctx->tune_scratch, (PK_MAX_RHS + 1) * sizeof(SolverScalars)));
+    PkParams<P> t = prm;
+    t.red.sc      = ctx->tune_scratch + PK_MAX_RHS;
+    t.red.result  = ctx->tune_scratch[PK_MAX_RHS].aux;
+    for (int r = 0; r < t.nrhs; ++r) {
+        t.r[r].sc     = ctx->tune_scratch + r;
+        t.r[r].result = nullptr;
+    }
+    c2q_ctx::TuneEntry e{0, {0, 0, 0, 0}};
+    float best = 0;
+    for (int c = 0; c < PK_CONFIGS; ++c) {
+        pk_dispatch<P>(t, c, nl, epi, dot, blocks, ctx->stream);
+        C2Q_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
+        pk_dispatch<P>(t, c, nl, epi, dot, blocks, ctx->stream);
+        pk_dispatch<P>(t, c, nl, epi, dot, blocks, ctx->stream);
+        C2Q_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
+        C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
+        C2Q_CUDA(ctx, cudaGetLastError());
+        float ms = 0;
+        C2Q_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        e.us[c] = 500.0f * ms;
+        if (c == 0 || e.us[c] < best) {
+            best  = e.us[c];
+            e.cfg = c;
+        }
+        ctx->launches += 3;
+    }
+    ctx->tune[key] = e;
+    *cfg           = e.cfg;
+    return C2Q_OK;
+}
 
 PkGeom pk_geom(const Geom& g)
 {
@@ -56,8 +134,8 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     const int nblk   = (prm.g.H + PK_THREADS - 1) / PK_THREADS;
     const int blocks = nblk * B.n;
     if (B.dot_mode) {
-        int rc = ensure_partials(ctx, blocks);
-        if (rc) return rc;
+        int rc0 = ensure_partials(ctx, blocks);
+        if (rc0) return rc0;
     }
     prm.red.partials = ctx->partials;
     prm.red.ticket   = ctx->ticket;
@@ -65,6 +143,10 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     prm.red.sc       = ctx->scalars;
     prm.red.fin      = B.fin;
     const bool r12   = gkind == G32R12 || gkind == G16R12;
+    const int nl     = r12 ? 6 : 9;
+    int cfg          = 0;
+    int rc           = pk_choose<P>(ctx, prm, nl, B.epi, B.dot_mode, blocks, &cfg);
+    if (rc) return rc;
     c2q_ctx::Timed tm{};
     if (ctx->profiling) {
         tm.a     = profile_event(ctx);
@@ -79,10 +161,7 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
                    (8.0 * lk + B.n * sp * (2.0 + (B.epi == EPI_AXPY ? 1.0 : 0.0) + (B.dot_mode == DOT_Y ? 1.0 : 0.0)));
         cudaEventRecord(tm.a, ctx->stream);
     }
-    if constexpr (P == 16)
-        pk_dispatch16(prm, B.epi, B.dot_mode, blocks, ctx->stream);
-    else
-        pk_dispatch32(prm, r12 ? 6 : 9, B.epi, B.dot_mode, blocks, ctx->stream);
+    pk_dispatch<P>(prm, cfg, nl, B.epi, B.dot_mode, blocks, ctx->stream);
     if (ctx->profiling) {
         cudaEventRecord(tm.b, ctx->stream);
         ctx->timed.push_back(tm);
@@ -113,3 +192,36 @@ int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B
 }
 
 }  // namespace c2q
+
+using namespace c2q;
+
+extern "C" {
+
+C2Q_EXPORT int c2q_ctx_set_autotune(c2q_ctx* ctx, int enable)
+{
+    if (!ctx) return C2Q_BAD_ARG;
+    ctx->autotune = enable != 0;
+    return C2Q_OK;
+}
+
+C2Q_EXPORT int c2q_ctx_tune_report(const c2q_ctx* ctx, char* buf, int len)
+{
+    if (!ctx) return C2Q_BAD_ARG;
+    std::string out;
+    char line[256];
+    for (const auto& kv : ctx->tune) {
+        const std::vector<int>& k = kv.first;
+        snprintf(line, sizeof line,
+                 "prec=%d links=%d epi=%d dot=%d phases=%d nrhs=%d sites=%d cfg=%d us=[%.1f, %.1f]\n", k[0],
+                 k[1] == 6 ? 12 : 18, k[2], k[3], k[4], k[5], k[6], kv.second.cfg, kv.second.us[0], kv.second.us[1]);
+        out += line;
+    }
+    if (buf && len > 0) {
+        const size_t n = out.size() < (size_t)len - 1 ? out.size() : (size_t)len - 1;
+        memcpy(buf, out.data(), n);
+        buf[n] = 0;
+    }
+    return (int)out.size() + 1;
+}
+
+}  // extern "C"

@@ -177,13 +177,24 @@ __device__ __forceinline__ void pk_channel(C2 acc[12], const C2 h[3], const C2 u
 // ring[(s * CH + c) * PK_THREADS + t]: consecutive threads read consecutive
 // 16-byte words.  Only the thread that copied a chunk reads it, so
 // cp.async.wait_group alone orders the copies and the reads.
+//
+// Launch configurations (CFG), chosen per launch shape by the autotuner of
+// pdslash.cu: ring depth STAGES and the resident blocks per SM (MINB) that
+// the register budget is fitted to.
+//   FP16: CFG 0 = 3 stages, 3 blocks/SM; CFG 1 = 2 stages, 4 blocks/SM
+//   FP32: CFG 0 = 2 stages, 2 blocks/SM; CFG 1 = 2 stages, 3 blocks/SM
+constexpr int PK_CONFIGS = 2;
 template <int P, int NL>
-struct PkStage {
-    static constexpr int SPC      = P == 16 ? 7 : 12;
-    static constexpr int LKC      = P == 16 ? 3 : NL;
-    static constexpr int CH       = SPC + LKC;
-    static constexpr int STAGES   = P == 16 ? 3 : 2;
-    static constexpr size_t BYTES = (size_t)STAGES * CH * 16 * PK_THREADS;
+struct PkChunks {
+    static constexpr int SPC = P == 16 ? 7 : 12;
+    static constexpr int LKC = P == 16 ? 3 : NL;
+    static constexpr int CH  = SPC + LKC;
+};
+template <int P, int NL, int CFG>
+struct PkStage : PkChunks<P, NL> {
+    static constexpr int STAGES   = (P == 16 && CFG == 0) ? 3 : 2;
+    static constexpr int MINB     = P == 16 ? (CFG == 0 ? 3 : 4) : (CFG == 0 ? 2 : 3);
+    static constexpr size_t BYTES = (size_t)STAGES * PkChunks<P, NL>::CH * 16 * PK_THREADS;
 };
 
 __device__ __forceinline__ void cp16(uint4* smem, const void* g)
@@ -217,7 +228,7 @@ __device__ __forceinline__ void stage_spinor(uint4* st, const void* d, const flo
 template <int P, int NL>
 __device__ __forceinline__ void stage_link(uint4* st, const char* links, int ss, int slot)
 {
-    constexpr int SPC = PkStage<P, NL>::SPC, LKC = PkStage<P, NL>::LKC;
+    constexpr int SPC = PkChunks<P, NL>::SPC, LKC = PkChunks<P, NL>::LKC;
     const uint4* p    = reinterpret_cast<const uint4*>(links) + slot;
 #pragma unroll
     for (int c = 0; c < LKC; ++c) cp16(st + (SPC + c) * PK_THREADS, p + (size_t)c * ss);
@@ -298,7 +309,7 @@ __device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, double phre,
     constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
     constexpr int c1 = BACK ? NegUnit<T::c1>::value : T::c1;
     C2 u[9];
-    staged_link<P, NL, BACK && SWP>(st + PkStage<P, NL>::SPC * PK_THREADS, u);
+    staged_link<P, NL, BACK && SWP>(st + PkChunks<P, NL>::SPC * PK_THREADS, u);
     Kc k;
     C2 h[3];
     if constexpr (P == 16) {
@@ -357,10 +368,10 @@ __host__ __device__ constexpr int pk_link_lanes()
     return P == 16 ? 3 : NL;
 }
 
-template <int P, int NL, int EPI, int DOT, int PH>
-__global__ void __launch_bounds__(PK_THREADS, P == 16 ? 3 : 2) pdslash_kernel(const PkParams<P> prm)
+template <int P, int NL, int EPI, int DOT, int PH, int CFG>
+__global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash_kernel(const PkParams<P> prm)
 {
-    using S = PkStage<P, NL>;
+    using S = PkStage<P, NL, CFG>;
     static_assert(S::STAGES == 2 || S::STAGES == 3, "the prologue below issues one or two stages");
     extern __shared__ uint4 ring[];
     uint4* mine     = ring + threadIdx.x;

@@ -89,6 +89,13 @@ class System:
         """Links read by the explicit operator calls: 18-real (default) or 12-real."""
         _check(self.lib.c2q_ctx_set_link_format(self.h, int(bool(rec12))), self.h, self.lib)
 
+    def tune_report(self) -> str:
+        """The launch configurations the autotuner chose, one line per launch shape."""
+        n = self.lib.c2q_ctx_tune_report(self.h, None, 0)
+        buf = C.create_string_buffer(max(n, 1))
+        self.lib.c2q_ctx_tune_report(self.h, buf, len(buf))
+        return buf.value.decode()
+
     def close(self):
         if getattr(self, "h", None):
             for child in list(self._children):

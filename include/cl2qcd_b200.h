@@ -192,6 +192,14 @@ C2Q_EXPORT int c2q_spinor_eo_convert(c2q_spinor_eo* out, const c2q_spinor_eo* in
  * apply_eo) read: 0 = 18-real (the reference's), 1 = 12-real with row-2
  * reconstruction.  FP16 operators always use 12-real FP16 links. */
 C2Q_EXPORT int c2q_ctx_set_link_format(c2q_ctx* ctx, int rec12);
+/* Autotuner of the reduced-precision sweeps (no counterpart in the reference):
+ * on by default (environment C2Q_AUTOTUNE=0 turns it off for new contexts);
+ * the first sweep of each launch shape times the kernel's launch
+ * configurations and keeps the fastest.  tune_report writes one line per
+ * shape into buf (NUL-terminated, truncated to len) and returns the length
+ * needed including the NUL. */
+C2Q_EXPORT int c2q_ctx_set_autotune(c2q_ctx* ctx, int enable);
+C2Q_EXPORT int c2q_ctx_tune_report(const c2q_ctx* ctx, char* buf, int len);
 /* convert_to_eoprec / convert_from_eoprec (physics/lattices/spinorfield_eo.cpp:372-410):
  * `full` is a host spinor[V]; `even` gets the sites with x+y+z+t even (FP64 fields). */
 C2Q_EXPORT int c2q_convert_to_eoprec(c2q_spinor_eo* even, c2q_spinor_eo* odd, const double* full);
