@@ -65,6 +65,8 @@ struct c2q_ctx {
     std::map<std::vector<int>, TuneEntry> tune;
     c2q::SolverScalars* tune_scratch = nullptr;  // reductions of tuning launches land here
     bool autotune = true;
+    // pinned ring of the batched solvers: 4 slots x 16 right-hand sides x 4 doubles
+    double* batch_ring = nullptr;
 };
 
 struct c2q_gauge {
@@ -168,6 +170,13 @@ struct PkBatch {
     int fin = FIN_STORE_RESULT;
 };
 int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B);
+// Batched fermion matrix on reduced-precision fields: out[r] = A in[r] for
+// r < n, tmp1/tmp2 per right-hand side; the last sweep optionally reduces
+// <y[r], out[r]> into sc[r] with finisher `fin`.
+int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out, const c2q_gauge* g, int gkind,
+                         const c2q_spinor_eo* const* in, double kappa, double mubar, int action,
+                         c2q_spinor_eo* const* tmp1, c2q_spinor_eo* const* tmp2, int dot_mode,
+                         const c2q_spinor_eo* const* y, int fin, SolverScalars* const* sc, int* sweeps);
 // an event for per-launch profiling (from the context's pool)
 cudaEvent_t profile_event(c2q_ctx* ctx);
 

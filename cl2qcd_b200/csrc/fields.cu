@@ -697,6 +697,7 @@ C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx)
     cudaFree(ctx->partials);
     cudaFree(ctx->ticket);
     if (ctx->tune_scratch) cudaFree(ctx->tune_scratch);
+    if (ctx->batch_ring) cudaFreeHost(ctx->batch_ring);
     cudaFree(ctx->red_result);
     cudaFree(ctx->scalars);
     cudaFree(ctx->staging);

@@ -191,6 +191,86 @@ int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B
     return P == 32 ? pk_launch<32>(ctx, g, gkind, B) : pk_launch<16>(ctx, g, gkind, B);
 }
 
+// Fermion matrices on a batch of reduced-precision right-hand sides (the
+// batched form of apply_operator in fields.cu): every sweep is one launch
+// over all right-hand sides.
+static int aee_sweeps_batch(c2q_ctx* ctx, int n, c2q_spinor_eo* const* out, const c2q_gauge* g, int gkind,
+                            const c2q_spinor_eo* const* in, double kappa, double mubar, int action, int minus, int g5,
+                            c2q_spinor_eo* const* tmp, int dot_mode, const c2q_spinor_eo* const* y, int fin,
+                            SolverScalars* const* sc)
+{
+    const bool tm = action == C2Q_ACTION_TWISTEDMASS;
+    PkBatch B;
+    B.n          = n;
+    B.kappa      = kappa;
+    B.out_parity = 0;  // ODD: the even sites
+    B.epi        = tm ? EPI_DIAG : EPI_PLAIN;
+    B.e          = tm ? diag_epi(mubar, minus ? C2Q_DIAG_M_TM_INVERSE_MINUS : C2Q_DIAG_M_TM_INVERSE, 0)
+                      : EpiArgs{1, 0, 1, 0, 0};
+    for (int r = 0; r < n; ++r) {
+        B.out[r] = tmp[r];
+        B.in[r]  = in[r];
+    }
+    int rc = launch_pdslash(ctx, g, gkind, B);
+    if (rc) return rc;
+    PkBatch C;
+    C.n          = n;
+    C.kappa      = kappa;
+    C.out_parity = 1;  // EVEN: the odd sites
+    C.epi        = EPI_AXPY;
+    C.e          = tm ? diag_epi(mubar, minus ? C2Q_DIAG_M_TM_MINUS : C2Q_DIAG_M_TM, g5) : EpiArgs{1, 0, 1, 0, g5};
+    C.dot_mode   = dot_mode;
+    C.fin        = fin;
+    for (int r = 0; r < n; ++r) {
+        C.out[r] = out[r];
+        C.in[r]  = tmp[r];
+        C.x[r]   = in[r];
+        C.y[r]   = y ? y[r] : nullptr;
+        C.sc[r]  = sc ? sc[r] : nullptr;
+    }
+    return launch_pdslash(ctx, g, gkind, C);
+}
+
+int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out, const c2q_gauge* g, int gkind,
+                         const c2q_spinor_eo* const* in, double kappa, double mubar, int action,
+                         c2q_spinor_eo* const* tmp1, c2q_spinor_eo* const* tmp2, int dot_mode,
+                         const c2q_spinor_eo* const* y, int fin, SolverScalars* const* sc, int* sweeps)
+{
+    if (action != C2Q_ACTION_WILSON && action != C2Q_ACTION_TWISTEDMASS)
+        return fail(ctx, C2Q_BAD_ARG, "unknown fermion action (wilson or twistedmass)");
+    int rc = 0;
+    switch (op) {
+        case C2Q_OP_AEE:
+            rc = aee_sweeps_batch(ctx, n, out, g, gkind, in, kappa, mubar, action, 0, 0, tmp1, dot_mode, y, fin, sc);
+            break;
+        case C2Q_OP_AEE_MINUS:
+            rc = aee_sweeps_batch(ctx, n, out, g, gkind, in, kappa, mubar, action, 1, 0, tmp1, dot_mode, y, fin, sc);
+            break;
+        case C2Q_OP_QPLUS_EO:
+        case C2Q_OP_AEE_AND_GAMMA5_EO:
+            rc = aee_sweeps_batch(ctx, n, out, g, gkind, in, kappa, mubar, action, 0, 1, tmp1, dot_mode, y, fin, sc);
+            break;
+        case C2Q_OP_QMINUS_EO:
+        case C2Q_OP_AEE_MINUS_AND_GAMMA5_EO:
+            rc = aee_sweeps_batch(ctx, n, out, g, gkind, in, kappa, mubar, action, 1, 1, tmp1, dot_mode, y, fin, sc);
+            break;
+        case C2Q_OP_QPLUSQMINUS_EO: {
+            const c2q_spinor_eo* mid[PK_MAX_RHS];
+            for (int r = 0; r < n; ++r) mid[r] = tmp2[r];
+            rc = aee_sweeps_batch(ctx, n, tmp2, g, gkind, in, kappa, mubar, action, 1, 1, tmp1, DOT_NONE, nullptr,
+                                  FIN_STORE_RESULT, nullptr);
+            if (!rc)
+                rc = aee_sweeps_batch(ctx, n, out, g, gkind, mid, kappa, mubar, action, 0, 1, tmp1, dot_mode, y, fin,
+                                      sc);
+            if (sweeps) *sweeps += 2;
+            break;
+        }
+        default: return fail(ctx, C2Q_BAD_ARG, "unknown eo fermion matrix");
+    }
+    if (sweeps) *sweeps += 2;
+    return rc;
+}
+
 }  // namespace c2q
 
 using namespace c2q;

@@ -439,129 +439,270 @@ int accumulate(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* xs)
     return C2Q_OK;
 }
 
+// Mixed-precision CG on a batch of right-hand sides that share the operator:
+// the right-hand sides iterate in lockstep (every sweep and vector update is
+// one launch over the active ones, so each link is read once per batch), each
+// with its own device scalars, its own pipelined residual monitoring and its
+// own FP64 reliable updates, and leaves the batch when it converges.  With
+// use_graph the iterations run as a captured CUDA graph (recaptured whenever
+// the set of active right-hand sides changes).  One right-hand side is the
+// plain mixed-precision CG.
+struct RhsState {
+    double b2 = 0, thr = 0, r2 = 0, resid = 0, maxrr = 0, r2_confirmed = -1;
+    int status = C2Q_DID_NOT_SOLVE, iters = 0, reliable = 0, skip_upto = -1, sweeps = 0;
+    bool active = false;
+};
+
+struct BatchGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> set;
+    long long kernels = 0;
+    ~BatchGraph() { reset(); }
+    void reset()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        set.clear();
+    }
+};
+
 template <int PB>
-int cg_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
-             double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
+int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gauge* g, const c2q_spinor_eo* const* b,
+                   int n, double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* reps)
 {
+    if (n < 1 || n > PK_MAX_RHS) return fail(ctx, C2Q_BAD_ARG, "batch size must be 1..16");
+    const c2q_lattice& lat = x[0]->lat;
     Fields F;
-    int rc = make_fields(ctx, x->lat, 64, 3, F, 0);  // r64, t1_64, t2_64
-    if (!rc) rc = make_fields(ctx, x->lat, 32, 2, F, 3);  // rs, xs
-    if (!rc) rc = make_fields(ctx, x->lat, PB, 4, F, 5);  // p, v, t1, t2
+    int rc = make_fields(ctx, lat, 64, 3, F, 0);                // r64, a64, b64 (reliable updates)
+    if (!rc) rc = make_fields(ctx, lat, 32, 2 * n, F, 3);        // rs, xs per right-hand side
+    if (!rc) rc = make_fields(ctx, lat, PB, 4 * n, F, 3 + 2 * n);  // p, v, t1, t2 per right-hand side
     if (rc) return rc;
     c2q_spinor_eo *r64 = &F.f[0], *a64 = &F.f[1], *b64 = &F.f[2];
-    c2q_spinor_eo *rs = &F.f[3], *xs = &F.f[4];
-    c2q_spinor_eo *p = &F.f[5], *v = &F.f[6], *t1 = &F.f[7], *t2 = &F.f[8];
-    const int gk   = gkind_for(PB, P->use_rec12 || PB == 16);
-    rc             = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
+    c2q_spinor_eo *rs[PK_MAX_RHS], *xs[PK_MAX_RHS], *p[PK_MAX_RHS], *v[PK_MAX_RHS], *t1[PK_MAX_RHS],
+        *t2[PK_MAX_RHS];
+    for (int k = 0; k < n; ++k) {
+        rs[k] = &F.f[3 + 2 * k];
+        xs[k] = &F.f[4 + 2 * k];
+        p[k]  = &F.f[3 + 2 * n + 4 * k];
+        v[k]  = &F.f[4 + 2 * n + 4 * k];
+        t1[k] = &F.f[5 + 2 * n + 4 * k];
+        t2[k] = &F.f[6 + 2 * n + 4 * k];
+    }
+    const int gk = gkind_for(PB, P->use_rec12 || PB == 16);
+    rc           = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
     if (rc) return rc;
+    SolverScalars* dsc = nullptr;
+    C2Q_CUDA(ctx, cudaMallocAsync(&dsc, n * sizeof(SolverScalars), ctx->stream));
+    struct Free {
+        c2q_ctx* c;
+        void* q;
+        ~Free() { cudaFreeAsync(q, c->stream); }
+    } free_dsc{ctx, dsc};
+    C2Q_CUDA(ctx, cudaMemsetAsync(dsc, 0, n * sizeof(SolverScalars), ctx->stream));
+    if (!ctx->batch_ring) C2Q_CUDA(ctx, cudaMallocHost(&ctx->batch_ring, 4 * PK_MAX_RHS * 4 * sizeof(double)));
     const double delta = P->reliable_delta > 0 ? P->reliable_delta : 0.1;
-    int sweeps         = 0, reliable = 0;
     SolveClock clock(ctx);
 
-    double b2 = 0;
-    rc        = saxpy_norm(ctx, r64, Cx{0, 0}, b, b, FIN_STORE_RESULT, &b2);
-    if (rc) return rc;
-    const double thr = stop_threshold(P, b2);
-    double r2        = 0, x2 = 0;
-    rc               = norm2(ctx, x, &x2);
-    if (rc) return rc;
-    if (x2 == 0.0) {
-        // r = b - A 0 = b: no operator application needed
-        rc = copy_field(ctx, r64, b);
-        r2 = b2;
-    } else {
-        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
-    }
-    if (rc) return rc;
-    int iter = 0, status = C2Q_DID_NOT_SOLVE;
-    double resid = r2, r2_confirmed = -1.0;
-    if (r2 < thr) {
-        status       = 0;
-        r2_confirmed = r2;
-    } else {
-        rc = launch_convert(ctx, rs, r64);
-        if (!rc) rc = c2q_spinor_eo_zero(xs);
-        if (!rc) rc = launch_convert(ctx, p, rs);
-        SolverScalars s0{};
-        s0.omega[0] = r2;
-        if (!rc) rc = write_sc(ctx, s0);
+    auto write_one = [&](int k, const SolverScalars& h) -> int {
+        memcpy(ctx->host_pinned, &h, sizeof(SolverScalars));
+        C2Q_CUDA(ctx, cudaMemcpyAsync(dsc + k, ctx->host_pinned, sizeof(SolverScalars), cudaMemcpyHostToDevice,
+                                      ctx->stream));
+        C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        return C2Q_OK;
+    };
+    auto read_one = [&](int k, SolverScalars* h) -> int {
+        C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, dsc + k, sizeof(SolverScalars), cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        memcpy(h, ctx->host_pinned, sizeof(SolverScalars));
+        return C2Q_OK;
+    };
+
+    // ---- initial residuals
+    RhsState S[PK_MAX_RHS];
+    for (int k = 0; k < n; ++k) {
+        RhsState& s = S[k];
+        rc          = saxpy_norm(ctx, r64, Cx{0, 0}, b[k], b[k], FIN_STORE_RESULT, &s.b2);
         if (rc) return rc;
-        double maxrr = std::sqrt(r2);
-        // Pipelined residual monitoring: every iteration copies |r|^2 into a
-        // pinned ring slot and records an event; the host reads iteration k-1
-        // while iteration k runs, so the GPU never waits for the host.  A
-        // decision taken on iteration k-1 is applied after iteration k.
-        ResidRing ring(ctx);
-        int skip_upto = -1;  // ring entries <= this index predate the last reliable update
-        for (iter = 0; iter < P->cgmax; ++iter) {
-            if (iter > 0) {
-                rc = mix_p<PB>(ctx, p, rs);  // p = r + beta p (beta of the previous iteration)
-                if (rc) return rc;
+        s.thr     = stop_threshold(P, s.b2);
+        double x2 = 0;
+        rc        = norm2(ctx, x[k], &x2);
+        if (rc) return rc;
+        if (x2 == 0.0) {  // r = b - A 0 = b
+            rc   = launch_convert(ctx, rs[k], b[k]);
+            s.r2 = s.b2;
+        } else {
+            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps);
+            if (!rc) rc = launch_convert(ctx, rs[k], r64);
+        }
+        if (rc) return rc;
+        s.resid = s.r2;
+        if (s.r2 < s.thr) {
+            s.status       = 0;
+            s.r2_confirmed = s.r2;
+            continue;
+        }
+        rc = c2q_spinor_eo_zero(xs[k]);
+        if (!rc) rc = launch_convert(ctx, p[k], rs[k]);
+        SolverScalars h0{};
+        h0.omega[0] = s.r2;
+        if (!rc) rc = write_one(k, h0);
+        if (rc) return rc;
+        s.maxrr  = std::sqrt(s.r2);
+        s.active = true;
+    }
+
+    // ---- iterations
+    const int per_apply = op == C2Q_OP_QPLUSQMINUS_EO ? 4 : 2;
+    const bool graphs   = P->use_graph && !ctx->profiling;
+    BatchGraph graph;
+    auto body = [&](const std::vector<int>& A, bool with_p) -> int {
+        const int m = (int)A.size();
+        MixBatch MB;
+        MB.n = m;
+        c2q_spinor_eo *outs[PK_MAX_RHS], *T1[PK_MAX_RHS], *T2[PK_MAX_RHS];
+        const c2q_spinor_eo* ins[PK_MAX_RHS];
+        SolverScalars* scs[PK_MAX_RHS];
+        for (int i = 0; i < m; ++i) {
+            const int k = A[i];
+            MB.xs[i]    = xs[k];
+            MB.rs[i]    = rs[k];
+            MB.p[i]     = p[k];
+            MB.v[i]     = v[k];
+            MB.sc[i]    = dsc + k;
+            outs[i]     = v[k];
+            ins[i]      = p[k];
+            scs[i]      = dsc + k;
+            T1[i]       = t1[k];
+            T2[i]       = t2[k];
+        }
+        int e = with_p ? mix_p_batch<PB>(ctx, MB) : 0;  // p = r + beta p
+        if (!e)  // v = A p with (p, v) -> alpha
+            e = apply_operator_batch(ctx, op, m, outs, g, gk, ins, kappa, mubar, action, T1, T2, DOT_Y, ins,
+                                     FIN_CG_ALPHA, scs, nullptr);
+        if (!e) e = mix_update_batch<PB>(ctx, MB);  // x += alpha p, r -= alpha v, |r|^2 -> beta
+        return e;
+    };
+    // Pipelined residual monitoring: every iteration copies |r|^2 and the
+    // division flag of all right-hand sides into a pinned ring slot and
+    // records an event; the host reads iteration k-1 while iteration k runs
+    // and applies its decisions after iteration k.
+    std::vector<int> hist[4], act;
+    int iter = 0;
+    for (iter = 0; iter < P->cgmax; ++iter) {
+        act.clear();
+        for (int k = 0; k < n; ++k)
+            if (S[k].active) act.push_back(k);
+        if (act.empty()) break;
+        hist[iter % 4] = act;
+        if (graphs && iter > 0) {
+            if (graph.set != act) {
+                graph.reset();
+                cudaGraph_t gr     = nullptr;
+                const long long l0 = ctx->launches;
+                C2Q_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+                const int eb         = body(act, true);
+                const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &gr);
+                if (eb) {
+                    if (gr) cudaGraphDestroy(gr);
+                    return eb;
+                }
+                C2Q_CUDA(ctx, ec);
+                const cudaError_t ei = cudaGraphInstantiate(&graph.exec, gr, 0);
+                cudaGraphDestroy(gr);
+                C2Q_CUDA(ctx, ei);
+                graph.set     = act;
+                graph.kernels = ctx->launches - l0;
+                ctx->launches = l0;
             }
-            DotSpec d;
-            d.mode = DOT_Y;
-            d.y    = p;
-            d.fin  = FIN_CG_ALPHA;
-            rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
-            if (!rc) rc = mix_update<PB>(ctx, xs, rs, p, v);
-            if (!rc) rc = ring.push(iter);
+            C2Q_CUDA(ctx, cudaGraphLaunch(graph.exec, ctx->stream));
+            ctx->launches += graph.kernels;
+        } else {
+            rc = body(act, iter > 0);
             if (rc) return rc;
-            if (iter == 0) continue;
-            double rprev = 0.0;
-            int bad      = 0;
-            rc           = ring.pop(iter - 1, &rprev, &bad);
-            if (rc) return rc;
-            if (iter - 1 <= skip_upto) continue;
-            resid = rprev;
+        }
+        for (int k : act) S[k].sweeps += per_apply;
+        double* slot = ctx->batch_ring + (size_t)(iter % 4) * PK_MAX_RHS * 4;
+        C2Q_CUDA(ctx, cudaMemcpy2DAsync(slot, 4 * sizeof(double), &dsc[0].resid, sizeof(SolverScalars),
+                                        4 * sizeof(double), n, cudaMemcpyDeviceToHost, ctx->stream));
+        C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[iter % 4], ctx->stream));
+        if (iter == 0) continue;
+        C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[(iter - 1) % 4]));
+        const double* prev = ctx->batch_ring + (size_t)((iter - 1) % 4) * PK_MAX_RHS * 4;
+        for (int k : hist[(iter - 1) % 4]) {
+            RhsState& s = S[k];
+            if (!s.active || iter - 1 <= s.skip_upto) continue;
+            const double resid = prev[4 * k];
+            int bad            = 0;
+            memcpy(&bad, prev + 4 * k + 3, sizeof(int));  // SolverScalars::flag follows resid and aux[2]
+            s.resid = resid;
             if (resid != resid || bad) {
-                status = C2Q_SOLVER_STUCK;
-                break;
+                s.status = C2Q_SOLVER_STUCK;
+                s.iters  = iter;
+                s.active = false;
+                rc       = accumulate(ctx, x[k], xs[k]);  // keep what was gained
+                if (rc) return rc;
+                continue;
             }
             const double rn = std::sqrt(resid);
-            if (rn > maxrr) maxrr = rn;
-            if (rn < delta * maxrr || resid < thr) {
+            if (rn > s.maxrr) s.maxrr = rn;
+            if (rn < delta * s.maxrr || resid < s.thr) {
                 // reliable update in FP64 after iteration `iter`
                 SolverScalars h;
-                rc = read_sc(ctx, &h);  // scalars of iteration `iter`
-                if (!rc) rc = accumulate(ctx, x, xs);
-                if (!rc) rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps);
+                rc = read_one(k, &h);
+                if (!rc) rc = accumulate(ctx, x[k], xs[k]);
+                if (!rc)
+                    rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps);
                 if (rc) return rc;
-                ++reliable;
-                resid = r2;
-                if (r2 < thr) {
-                    status       = iter + 1;
-                    r2_confirmed = r2;
-                    break;
+                ++s.reliable;
+                s.resid = s.r2;
+                if (s.r2 < s.thr) {
+                    s.status       = iter + 1;
+                    s.iters        = iter + 1;
+                    s.r2_confirmed = s.r2;
+                    s.active       = false;
+                    continue;
                 }
-                rc = launch_convert(ctx, rs, r64);
+                rc = launch_convert(ctx, rs[k], r64);
                 if (rc) return rc;
-                maxrr = std::sqrt(r2);
+                s.maxrr = std::sqrt(s.r2);
                 // keep the search direction; rescale beta to the true residual
-                h.beta[0] *= r2 / h.resid;
-                h.beta[1] *= r2 / h.resid;
-                h.omega[0] = r2;
+                h.beta[0] *= s.r2 / h.resid;
+                h.beta[1] *= s.r2 / h.resid;
+                h.omega[0] = s.r2;
                 h.omega[1] = 0.0;
-                h.resid    = r2;
-                rc         = write_sc(ctx, h);
+                h.resid    = s.r2;
+                rc         = write_one(k, h);
                 if (rc) return rc;
-                skip_upto = iter;
+                s.skip_upto = iter;
             }
         }
-        if (status == C2Q_DID_NOT_SOLVE || status == C2Q_SOLVER_STUCK) {
-            // keep what was gained
-            int rc2 = accumulate(ctx, x, xs);
-            if (rc2) return rc2;
+    }
+    graph.reset();
+    for (int k = 0; k < n; ++k)
+        if (S[k].active) {  // out of iterations: keep what was gained
+            S[k].iters  = iter;
+            S[k].active = false;
+            rc          = accumulate(ctx, x[k], xs[k]);
+            if (rc) return rc;
         }
+    const double secs = clock.seconds();
+    int worst         = 0;
+    for (int k = 0; k < n; ++k) {
+        RhsState& s = S[k];
+        double r2t  = s.r2_confirmed;
+        if (r2t < 0) {
+            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &r2t, &s.sweeps);
+            if (rc) return rc;
+        }
+        finish_report(reps ? &reps[k] : nullptr, s.status, s.iters, s.reliable, s.resid,
+                      s.b2 > 0 ? std::sqrt(r2t / s.b2) : 0.0, secs, s.sweeps);
+        if (s.status < 0 && (worst == 0 || s.status == C2Q_SOLVER_STUCK)) worst = s.status;
     }
-    double r2t = r2_confirmed;
-    if (r2t < 0) {
-        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2t, &sweeps);
-        if (rc) return rc;
-    }
-    finish_report(rep, status, iter, reliable, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sweeps);
-    if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
-    if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "NAN occured in the mixed-precision CG residual");
-    return status;
+    if (worst == C2Q_DID_NOT_SOLVE) fail(ctx, worst, "Solver did not solve in solverMaxIterations iterations");
+    if (worst == C2Q_SOLVER_STUCK) fail(ctx, worst, "NAN occured in the mixed-precision CG residual");
+    if (worst < 0) return worst;
+    return n == 1 ? S[0].status : C2Q_OK;
 }
 
 // ------------------------------------------------------------- BiCGStab
@@ -780,8 +921,8 @@ C2Q_EXPORT int c2q_cg(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_sp
     if (x == b) return fail(ctx, C2Q_BAD_ARG, "solution and source must be different fields");
     switch (p->precision) {
         case 64: return cg_fp64(ctx, x, op, g, b, kappa, mubar, action, p, report);
-        case 32: return cg_mixed<32>(ctx, x, op, g, b, kappa, mubar, action, p, report);
-        default: return cg_mixed<16>(ctx, x, op, g, b, kappa, mubar, action, p, report);
+        case 32: return cg_mixed_batch<32>(ctx, &x, op, g, &b, 1, kappa, mubar, action, p, report);
+        default: return cg_mixed_batch<16>(ctx, &x, op, g, &b, 1, kappa, mubar, action, p, report);
     }
 }
 
@@ -800,13 +941,37 @@ C2Q_EXPORT int c2q_cg_multi(c2q_spinor_eo* const* x, int op, const c2q_gauge* g,
                             int nrhs, double kappa, double mubar, int action, const c2q_solver_params* p,
                             c2q_solve_report* reports)
 {
-    if (!x || !b || nrhs <= 0) return C2Q_BAD_ARG;
-    int worst = 0;
+    if (!x || !b || nrhs <= 0 || !x[0]) return C2Q_BAD_ARG;
+    c2q_ctx* ctx = x[0]->ctx;
+    int rc       = 0;
     for (int k = 0; k < nrhs; ++k) {
-        int rc = c2q_cg(x[k], op, g, b[k], kappa, mubar, action, p, reports ? &reports[k] : nullptr);
-        if (rc < 0 && (worst >= 0 || rc < worst)) worst = rc;
+        if (!x[k] || !validate(ctx, x[k], g, b[k], p, &rc)) return rc ? rc : C2Q_BAD_ARG;
+        if (x[k]->ctx != ctx || !same_lattice(x[k]->lat, x[0]->lat))
+            return fail(ctx, C2Q_BAD_ARG, "all right-hand sides must share the context and lattice");
+        for (int l = 0; l < nrhs; ++l)
+            if (x[k] == b[l] || (l != k && x[k] == x[l]))
+                return fail(ctx, C2Q_BAD_ARG, "solutions must be distinct fields, distinct from the sources");
     }
-    return worst < 0 ? worst : C2Q_OK;
+    int worst = 0;
+    if (p->precision == 64) {  // the reference's FP64 CG, one right-hand side after the other
+        for (int k = 0; k < nrhs; ++k) {
+            rc = c2q_cg(x[k], op, g, b[k], kappa, mubar, action, p, reports ? &reports[k] : nullptr);
+            if (rc < 0 && (worst == 0 || rc == C2Q_SOLVER_STUCK)) worst = rc;
+        }
+        return worst;
+    }
+    // mixed precision: batches of up to 16 right-hand sides share every sweep
+    for (int k0 = 0; k0 < nrhs; k0 += PK_MAX_RHS) {
+        const int m = std::min(PK_MAX_RHS, nrhs - k0);
+        rc          = p->precision == 32
+                          ? cg_mixed_batch<32>(ctx, x + k0, op, g, b + k0, m, kappa, mubar, action, p,
+                                               reports ? reports + k0 : nullptr)
+                          : cg_mixed_batch<16>(ctx, x + k0, op, g, b + k0, m, kappa, mubar, action, p,
+                                               reports ? reports + k0 : nullptr);
+        if (rc < 0 && rc != C2Q_SOLVER_STUCK && rc != C2Q_DID_NOT_SOLVE) return rc;
+        if (rc < 0 && (worst == 0 || rc == C2Q_SOLVER_STUCK)) worst = rc;
+    }
+    return worst;
 }
 
 // Eo branch of invert_M_nf2_upperflavour (physics/algorithms/inversion.cpp:129-236).

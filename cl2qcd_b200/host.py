@@ -418,6 +418,43 @@ def cg(x, A, gf, b, params: SolverParameters, add: AdditionalParameters, report:
     return _solve(x.system.lib.c2q_cg, x, A, gf, b, params, add, report)
 
 
+def cg_multi(xs, A, gf, bs, params: SolverParameters, add: AdditionalParameters,
+             reports: list | None = None) -> list:
+    """CG on A x[k] = b[k] for every k.  With precision 32 or 16 up to 16
+    right-hand sides iterate as one batch whose sweeps read each link once;
+    each right-hand side keeps its own scalars, reliable updates and stopping
+    test (the same semantics as cg).  Returns the iteration counts."""
+    n = len(xs)
+    assert n == len(bs) and n > 0
+    lib = xs[0].system.lib
+    p = params.c()
+    ax = (C.c_void_p * n)(*[x.h for x in xs])
+    ab = (C.c_void_p * n)(*[b.h for b in bs])
+    reps = (L.CSolveReport * n)()
+    rc = lib.c2q_cg_multi(ax, A.OP, gf.h, ab, n, add.kappa, add.mubar, A.action, C.byref(p), reps)
+    out = [r.as_dict() for r in reps]
+    if reports is not None:
+        reports.clear()
+        reports.extend(out)
+    msg = (lib.c2q_last_error(xs[0].system.h) or b"").decode()
+    if rc == L.SOLVER_STUCK:
+        raise SolverStuck(max(r["iterations"] for r in out), msg)
+    if rc == L.DID_NOT_SOLVE:
+        raise SolverDidNotSolve(max(r["iterations"] for r in out), msg)
+    _check(rc, xs[0].system.h, lib)
+    return [r["iterations"] for r in out]
+
+
+def point_source(n_sites: int, k: int) -> np.ndarray:
+    """Spin-colour point source k (spin k % 4, colour k // 4) at the origin, as
+    an eo field: the origin is eo site 0 of the even sites
+    (ocl_kernel/operations_geometry.cl:476-489, spinorfield_point_source.cl:23-75)."""
+    out = np.zeros((n_sites, 24))
+    spin, colour = k % 4, k // 4
+    out[0, 2 * (3 * spin + colour)] = 1.0
+    return out
+
+
 def bicgstab(x, A, gf, b, params: SolverParameters, add: AdditionalParameters, report: dict | None = None) -> int:
     return _solve(x.system.lib.c2q_bicgstab, x, A, gf, b, params, add, report)
 
