@@ -65,6 +65,7 @@ struct c2q_ctx {
     std::map<std::vector<int>, TuneEntry> tune;
     c2q::SolverScalars* tune_scratch = nullptr;  // reductions of tuning launches land here
     bool autotune = true;
+    int sm_count  = 0;
     // pinned ring of the batched solvers: 4 slots x 16 right-hand sides x 4 doubles
     double* batch_ring = nullptr;
 };
@@ -171,8 +172,9 @@ struct PkBatch {
 };
 int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B);
 // Batched fermion matrix on reduced-precision fields: out[r] = A in[r] for
-// r < n, tmp1/tmp2 per right-hand side; the last sweep optionally reduces
-// <y[r], out[r]> into sc[r] with finisher `fin`.
+// r < n, tmp1/tmp2 per right-hand side; optionally reduces <y[r], out[r]>
+// into sc[r] with finisher `fin` (for QplusQminus_eo with y = in, as
+// |Qminus_eo in|^2, which equals it because Qplus_eo = Qminus_eo^dagger).
 int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out, const c2q_gauge* g, int gkind,
                          const c2q_spinor_eo* const* in, double kappa, double mubar, int action,
                          c2q_spinor_eo* const* tmp1, c2q_spinor_eo* const* tmp2, int dot_mode,

@@ -57,7 +57,9 @@ __device__ __forceinline__ C2 caxpy2(C2 a, float2 cre, float2 cim, float2 ncim, 
     return C2{fma2(b.re, cre, fma2(b.im, ncim, a.re)), fma2(b.im, cre, fma2(b.re, cim, a.im))};
 }
 
-// x += alpha p ; r -= alpha v ; |r|^2 -> FIN_CG_BETA of the right-hand side
+// r -= alpha v ; |r|^2 -> FIN_CG_BETA of the right-hand side.  The matching
+// solution update x += alpha p is deferred to the next mix_p (which reads p
+// anyway) or to the reliable-update accumulation.
 template <int PB>
 __global__ void __launch_bounds__(MIX_THREADS) mix_update_kernel(const MixArgs A)
 {
@@ -71,17 +73,9 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_update_kernel(const MixArgs A
         const float ar = (float)F.sc->alpha[0], ai = (float)F.sc->alpha[1];
         C2 a[12], b[12];
         float2 bs;
-        SlotF32::load(F.x, A.ss, j, a);
-        mix_load<PB>(F.p, F.p_norm, A.ss, j, b, &bs);
-        float2 cr = mul2(bc2(ar), bs), ci = mul2(bc2(ai), bs), nci = mul2(bc2(-ai), bs);
-#pragma unroll
-        for (int c = 0; c < 12; ++c) a[c] = caxpy2(a[c], cr, ci, nci, b[c]);
-        SlotF32::store(F.x, A.ss, j, a);
         SlotF32::load(F.r, A.ss, j, a);
         mix_load<PB>(F.v, F.v_norm, A.ss, j, b, &bs);
-        cr  = mul2(bc2(-ar), bs);
-        ci  = mul2(bc2(-ai), bs);
-        nci = mul2(bc2(ai), bs);
+        const float2 cr = mul2(bc2(-ar), bs), ci = mul2(bc2(-ai), bs), nci = mul2(bc2(ai), bs);
 #pragma unroll
         for (int c = 0; c < 12; ++c) {
             a[c] = caxpy2(a[c], cr, ci, nci, b[c]);
@@ -97,7 +91,7 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_update_kernel(const MixArgs A
     finish_reduction<2>(dv, ra, smem, rhs, nrhs);
 }
 
-// p = r + beta p
+// x += alpha p (the previous iteration's deferred update), then p = r + beta p
 template <int PB>
 __global__ void __launch_bounds__(MIX_THREADS) mix_p_kernel(const MixArgs A)
 {
@@ -107,34 +101,52 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_p_kernel(const MixArgs A)
     const int j        = blk * MIX_THREADS + threadIdx.x;
     const MixFields& F = A.f[rhs];
     if (j >= A.H) return;
+    const float ar = (float)F.sc->alpha[0], ai = (float)F.sc->alpha[1];
     const float br = (float)F.sc->beta[0], bi = (float)F.sc->beta[1];
     C2 p[12], r[12];
     float2 ps;
     mix_load<PB>(F.p, F.p_norm, A.ss, j, p, &ps);
+    SlotF32::load(F.x, A.ss, j, r);
+    float2 cr = mul2(bc2(ar), ps), ci = mul2(bc2(ai), ps), nci = mul2(bc2(-ai), ps);
+#pragma unroll
+    for (int c = 0; c < 12; ++c) r[c] = caxpy2(r[c], cr, ci, nci, p[c]);
+    SlotF32::store(F.x, A.ss, j, r);
     SlotF32::load(F.r, A.ss, j, r);
-    const float2 cr = mul2(bc2(br), ps), ci = mul2(bc2(bi), ps), nci = mul2(bc2(-bi), ps);
+    cr  = mul2(bc2(br), ps);
+    ci  = mul2(bc2(bi), ps);
+    nci = mul2(bc2(-bi), ps);
 #pragma unroll
     for (int c = 0; c < 12; ++c) p[c] = caxpy2(r[c], cr, ci, nci, p[c]);
     mix_store<PB>(F.p, F.p_norm, A.ss, j, p);
 }
 
-// x64 = x64 + (double) x_s ; x_s = 0   (reliable update accumulation in FP64)
-template <int PA>
-__global__ void __launch_bounds__(BLAS_THREADS) accumulate_kernel(SpinorPtr<64> x, SpinorPtr<PA> xs, int n, int stride)
+// x64 = x64 + (double) (x_s + alpha p) ; x_s = 0   (reliable update
+// accumulation in FP64, including the deferred update of the last iteration;
+// `sc` null: x_s only)
+template <int PB>
+__global__ void __launch_bounds__(BLAS_THREADS) accumulate_kernel(SpinorPtr<64> x, SpinorPtr<32> xs, SpinorPtr<PB> p,
+                                                                  const SolverScalars* sc, int n, int stride)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     Cplx<double> a[12];
     Cplx<float> b[12];
     SpinorIO<64>::load(x, stride, i, a);
-    SpinorIO<PA>::load(xs, stride, i, b);
+    SpinorIO<32>::load(xs, stride, i, b);
+    if (sc) {
+        Cplx<float> q[12];
+        SpinorIO<PB>::load(p, stride, i, q);
+        const Cplx<float> al = cmk<float>((float)sc->alpha[0], (float)sc->alpha[1]);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) b[k] = b[k] + cmul(al, q[k]);
+    }
 #pragma unroll
     for (int k = 0; k < 12; ++k) {
         a[k] = a[k] + cmk<double>((double)b[k].re, (double)b[k].im);
         b[k] = cmk<float>(0.f, 0.f);
     }
     SpinorIO<64>::store(x, stride, i, a);
-    SpinorIO<PA>::store(xs, stride, i, b);
+    SpinorIO<32>::store(xs, stride, i, b);
 }
 
 }  // namespace c2q

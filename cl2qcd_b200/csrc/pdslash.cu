@@ -14,6 +14,43 @@ void pk_dispatch32_c1(const PkParams<32>& prm, int nl, int epi, int dot, int blo
 void pk_dispatch16_c0(const PkParams<16>& prm, int epi, int dot, int blocks, cudaStream_t s);
 void pk_dispatch16_c1(const PkParams<16>& prm, int epi, int dot, int blocks, cudaStream_t s);
 
+// Resident blocks per SM of a configuration: its launch bound, or what its
+// shared-memory ring leaves room for (228 KB per SM, 1 KB reserved per block).
+static int pk_blocks_per_sm(int P, int nl, int cfg)
+{
+    int minb     = 0;
+    size_t bytes = 0;
+    if (P == 16) {
+        minb  = cfg ? PkStage<16, 6, 1>::MINB : PkStage<16, 6, 0>::MINB;
+        bytes = cfg ? PkStage<16, 6, 1>::BYTES : PkStage<16, 6, 0>::BYTES;
+    } else if (nl == 6) {
+        minb  = cfg ? PkStage<32, 6, 1>::MINB : PkStage<32, 6, 0>::MINB;
+        bytes = cfg ? PkStage<32, 6, 1>::BYTES : PkStage<32, 6, 0>::BYTES;
+    } else {
+        minb  = cfg ? PkStage<32, 9, 1>::MINB : PkStage<32, 9, 0>::MINB;
+        bytes = cfg ? PkStage<32, 9, 1>::BYTES : PkStage<32, 9, 0>::BYTES;
+    }
+    const int by_smem = (int)((228u * 1024u) / (bytes + 1024u));
+    return minb < by_smem ? minb : by_smem;
+}
+
+// Grid of a launch: one block per tile, or (grid-stride) as many blocks per
+// right-hand side as the GPU holds resident at once.
+static int pk_grid(c2q_ctx* ctx, int P, int nl, int cfg, bool persistent, int ntiles, int nrhs)
+{
+    if (!persistent) return ntiles * nrhs;
+    if (ctx->sm_count <= 0) {
+        int n = 0;
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, ctx->device);
+        ctx->sm_count = n > 0 ? n : 148;
+    }
+    const int resident = pk_blocks_per_sm(P, nl, cfg) * ctx->sm_count;
+    int G              = (resident + nrhs - 1) / nrhs;
+    if (G > ntiles) G = ntiles;
+    if (G < 1) G = 1;
+    return G * nrhs;
+}
+
 template <int P>
 static void pk_dispatch(const PkParams<P>& prm, int cfg, int nl, int epi, int dot, int blocks, cudaStream_t s)
 {
@@ -38,8 +75,12 @@ static void pk_dispatch(const PkParams<P>& prm, int cfg, int nl, int epi, int do
 // idempotent (the output depends only on the inputs), so tuning does not
 // change results.  Shapes first met inside a graph capture use
 // configuration 0 and are not recorded.
+// A tuning choice c selects the kernel configuration c & 1 and the grid
+// (c >> 1: grid-stride over resident blocks instead of one block per tile).
+constexpr int PK_CHOICES = 2 * PK_CONFIGS;
+
 template <int P>
-static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int dot, int blocks, int* cfg)
+static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int dot, int* cfg)
 {
     *cfg = 0;
     if (!ctx->autotune) return C2Q_OK;
@@ -65,11 +106,12 @@ static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int 
     }
     c2q_ctx::TuneEntry e{0, {0, 0, 0, 0}};
     float best = 0;
-    for (int c = 0; c < PK_CONFIGS; ++c) {
-        pk_dispatch<P>(t, c, nl, epi, dot, blocks, ctx->stream);
+    for (int c = 0; c < PK_CHOICES; ++c) {
+        const int blocks = pk_grid(ctx, P, nl, c & 1, c >> 1, t.ntiles, t.nrhs);
+        pk_dispatch<P>(t, c & 1, nl, epi, dot, blocks, ctx->stream);
         C2Q_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-        pk_dispatch<P>(t, c, nl, epi, dot, blocks, ctx->stream);
-        pk_dispatch<P>(t, c, nl, epi, dot, blocks, ctx->stream);
+        pk_dispatch<P>(t, c & 1, nl, epi, dot, blocks, ctx->stream);
+        pk_dispatch<P>(t, c & 1, nl, epi, dot, blocks, ctx->stream);
         C2Q_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
         C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
         C2Q_CUDA(ctx, cudaGetLastError());
@@ -131,10 +173,9 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     if (P == 16) prm.c.scale *= 1.0 / (32767.0 * 32767.0);
     prm.e          = B.e;
     prm.out_parity = B.out_parity;
-    const int nblk   = (prm.g.H + PK_THREADS - 1) / PK_THREADS;
-    const int blocks = nblk * B.n;
-    if (B.dot_mode) {
-        int rc0 = ensure_partials(ctx, blocks);
+    prm.ntiles = (prm.g.H + PK_THREADS - 1) / PK_THREADS;
+    if (B.dot_mode) {  // one partial per tile and right-hand side
+        int rc0 = ensure_partials(ctx, (size_t)prm.ntiles * B.n);
         if (rc0) return rc0;
     }
     prm.red.partials = ctx->partials;
@@ -144,9 +185,11 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     prm.red.fin      = B.fin;
     const bool r12   = gkind == G32R12 || gkind == G16R12;
     const int nl     = r12 ? 6 : 9;
-    int cfg          = 0;
-    int rc           = pk_choose<P>(ctx, prm, nl, B.epi, B.dot_mode, blocks, &cfg);
+    int choice       = 0;
+    int rc           = pk_choose<P>(ctx, prm, nl, B.epi, B.dot_mode, &choice);
     if (rc) return rc;
+    const int cfg    = choice & 1;
+    const int blocks = pk_grid(ctx, P, nl, cfg, choice >> 1, prm.ntiles, B.n);
     c2q_ctx::Timed tm{};
     if (ctx->profiling) {
         tm.a     = profile_event(ctx);
@@ -256,12 +299,16 @@ int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out,
             break;
         case C2Q_OP_QPLUSQMINUS_EO: {
             const c2q_spinor_eo* mid[PK_MAX_RHS];
+            bool self = dot_mode == DOT_Y;
+            for (int r = 0; r < n && self; ++r) self = y && y[r] == in[r];
             for (int r = 0; r < n; ++r) mid[r] = tmp2[r];
-            rc = aee_sweeps_batch(ctx, n, tmp2, g, gkind, in, kappa, mubar, action, 1, 1, tmp1, DOT_NONE, nullptr,
-                                  FIN_STORE_RESULT, nullptr);
+            // <in, Q+ Q- in> = |Q- in|^2 (Qplus_eo is the adjoint of Qminus_eo):
+            // reduced from the intermediate in registers, with no operand read
+            rc = aee_sweeps_batch(ctx, n, tmp2, g, gkind, in, kappa, mubar, action, 1, 1, tmp1,
+                                  self ? DOT_SELF : DOT_NONE, nullptr, fin, sc);
             if (!rc)
-                rc = aee_sweeps_batch(ctx, n, out, g, gkind, mid, kappa, mubar, action, 0, 1, tmp1, dot_mode, y, fin,
-                                      sc);
+                rc = aee_sweeps_batch(ctx, n, out, g, gkind, mid, kappa, mubar, action, 0, 1, tmp1,
+                                      self ? DOT_NONE : dot_mode, y, fin, sc);
             if (sweeps) *sweeps += 2;
             break;
         }
@@ -292,8 +339,11 @@ C2Q_EXPORT int c2q_ctx_tune_report(const c2q_ctx* ctx, char* buf, int len)
     for (const auto& kv : ctx->tune) {
         const std::vector<int>& k = kv.first;
         snprintf(line, sizeof line,
-                 "prec=%d links=%d epi=%d dot=%d phases=%d nrhs=%d sites=%d cfg=%d us=[%.1f, %.1f]\n", k[0],
-                 k[1] == 6 ? 12 : 18, k[2], k[3], k[4], k[5], k[6], kv.second.cfg, kv.second.us[0], kv.second.us[1]);
+                 "prec=%d links=%d epi=%d dot=%d phases=%d nrhs=%d sites=%d choice=%d (config %d, %s grid) "
+                 "us=[%.1f, %.1f, %.1f, %.1f]\n",
+                 k[0], k[1] == 6 ? 12 : 18, k[2], k[3], k[4], k[5], k[6], kv.second.cfg, kv.second.cfg & 1,
+                 (kv.second.cfg >> 1) ? "grid-stride" : "per-tile", kv.second.us[0], kv.second.us[1], kv.second.us[2],
+                 kv.second.us[3]);
         out += line;
     }
     if (buf && len > 0) {

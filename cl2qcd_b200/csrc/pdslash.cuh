@@ -61,6 +61,7 @@ struct PkParams {
     HopCoef c;
     EpiArgs e;
     int out_parity;
+    int ntiles;  // tiles of PK_THREADS slots per right-hand side
     RedArgs red;
 };
 
@@ -379,8 +380,14 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
     const int nrhs  = prm.nrhs;
     const int rhs   = nrhs == 1 ? 0 : (int)(blockIdx.x % (unsigned)nrhs);
     const int blk   = nrhs == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nrhs);
-    const int j     = blk * PK_THREADS + threadIdx.x;
+    const int G     = (int)gridDim.x / nrhs;  // blocks per right-hand side
     const PkRhs& rr = prm.r[rhs];
+    __shared__ double smem[2 * 32];
+
+    // tiles of PK_THREADS slots; a block takes tiles blk, blk + G, ... (one
+    // tile per block unless the grid is sized to the resident blocks)
+    for (int tile = blk; tile < prm.ntiles; tile += G) {
+    const int j = tile * PK_THREADS + threadIdx.x;
     float2 dre = bc2(0.f), dim = bc2(0.f), dq = bc2(0.f);
 
     if (j < g.H) {
@@ -525,15 +532,18 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
             for (int c = 0; c < 12; ++c) dre = fma2(acc[c].re, acc[c].re, fma2(acc[c].im, acc[c].im, dre));
         }
     }
-    if (DOT != DOT_NONE) {
+    if (DOT != DOT_NONE) {  // one partial per tile, in tile order
         double dv[2] = {(double)dre.x + (double)dre.y,
                         ((double)dim.x - (double)dq.x) + ((double)dim.y - (double)dq.y)};
-        __shared__ double smem[2 * 32];
         block_sum<2>(dv, smem);
+        store_partial<2>(dv, prm.red, (size_t)tile * nrhs + rhs);
+    }
+    }  // tiles
+    if (DOT != DOT_NONE) {
         RedArgs ra = prm.red;
         if (rr.sc) ra.sc = rr.sc;
         if (rr.result) ra.result = rr.result;
-        finish_reduction<2>(dv, ra, smem, rhs, nrhs);
+        finish_group<2>(ra, smem, rhs, nrhs, prm.ntiles, G);
     }
 }
 

@@ -80,35 +80,59 @@ __device__ __forceinline__ void cdiv_store(double* out, const double* n, const d
     out[1] = (n[1] * d[0] - n[0] * d[1]) / norm;
 }
 
+// Partial `index` of a reduction (thread 0 holds the block sum).
+template <int NV>
+__device__ __forceinline__ void store_partial(const double v[NV], const RedArgs& ra, size_t index)
+{
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) ra.partials[index * NV + k] = v[k];
+}
+
 // Called by every thread of every block after block_sum (value in thread 0).
 // Batched launches reduce per group: block b belongs to group b % G (one
 // group per right-hand side), each group has its own ticket ra.ticket[grp]
 // and its last block sums that group's partials in block order.
 template <int NV>
 __device__ __forceinline__ void finish_reduction(const double v[NV], const RedArgs& ra, double* smem, int grp = 0,
-                                                 int G = 1)
+                                                 int G = 1);
+
+// The ticket and final sum of a group whose `nparts` partials sit at
+// partials[(m * G + grp) * NV], m < nparts, written by the `nblocks` blocks of
+// the group (grid-stride kernels write several partials per block).
+template <int NV>
+__device__ __forceinline__ void finish_group(const RedArgs& ra, double* smem, int grp, int G, int nparts, int nblocks)
 {
     __shared__ bool last;
-    const int nb = (int)gridDim.x / G;  // blocks of this group
     if (threadIdx.x == 0) {
-#pragma unroll
-        for (int k = 0; k < NV; ++k) ra.partials[(size_t)blockIdx.x * NV + k] = v[k];
         __threadfence();
         const unsigned t = atomicAdd(ra.ticket + grp, 1u);
-        last             = (t == (unsigned)nb - 1u);
+        last             = (t == (unsigned)nblocks - 1u);
     }
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // fixed-order sum of the group's partials: thread j takes a contiguous chunk
+    const int nb = nparts;
+    // fixed-order sum of the group's partials: thread j takes partials
+    // j, j + blockDim.x, ... in rounds of 8 independent loads (this block runs
+    // alone at the end of the kernel, so its load latency is not hidden)
     double acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0.0;
-    const int chunk = (nb + blockDim.x - 1) / blockDim.x;
-    const int lo = threadIdx.x * chunk, hi = min(nb, lo + chunk);
-    for (int m = lo; m < hi; ++m)
+    const int step = blockDim.x;
+    for (int m0 = threadIdx.x; m0 < nb; m0 += 8 * step) {
+        double t[8][NV];
 #pragma unroll
-        for (int k = 0; k < NV; ++k) acc[k] += __ldcg(ra.partials + ((size_t)m * G + grp) * NV + k);
+        for (int u = 0; u < 8; ++u) {
+            const int m = m0 + u * step;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) t[u][k] = m < nb ? __ldcg(ra.partials + ((size_t)m * G + grp) * NV + k) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) acc[k] += t[u][k];
+    }
     block_sum<NV>(acc, smem);
     if (threadIdx.x == 0) {
         ra.ticket[grp] = 0u;
@@ -142,6 +166,14 @@ __device__ __forceinline__ void finish_reduction(const double v[NV], const RedAr
         }
         __threadfence();
     }
+}
+
+template <int NV>
+__device__ __forceinline__ void finish_reduction(const double v[NV], const RedArgs& ra, double* smem, int grp, int G)
+{
+    store_partial<NV>(v, ra, blockIdx.x);
+    const int nb = (int)gridDim.x / G;  // blocks (= partials) of this group
+    finish_group<NV>(ra, smem, grp, G, nb, nb);
 }
 
 }  // namespace c2q

@@ -122,9 +122,9 @@ int copy_field(c2q_ctx* ctx, c2q_spinor_eo* to, const c2q_spinor_eo* from)
 // ||b - A x||^2 in FP64 (true residual); r receives b - A x.
 int true_residual(c2q_ctx* ctx, int op, const c2q_gauge* g, const c2q_spinor_eo* x, const c2q_spinor_eo* b,
                   double kappa, double mubar, int action, c2q_spinor_eo* r, c2q_spinor_eo* t1, c2q_spinor_eo* t2,
-                  double* r2, int* sweeps)
+                  double* r2, int* sweeps, int gk64 = G64)
 {
-    int rc = apply_operator(ctx, op, r, g, G64, x, kappa, mubar, action, t1, t2, DotSpec{}, sweeps);
+    int rc = apply_operator(ctx, op, r, g, gk64, x, kappa, mubar, action, t1, t2, DotSpec{}, sweeps);
     if (rc) return rc;
     return saxpy_norm(ctx, r, Cx{1, 0}, r, b, FIN_STORE_RESULT, r2);
 }
@@ -405,35 +405,13 @@ int mix_p_batch(c2q_ctx* ctx, const MixBatch& B)
     return C2Q_OK;
 }
 
+// x += x_s + alpha p (alpha from `sc`; sc null: x += x_s), x_s = 0
 template <int PB>
-int mix_update(c2q_ctx* ctx, c2q_spinor_eo* xs, c2q_spinor_eo* rs, c2q_spinor_eo* p, const c2q_spinor_eo* v)
-{
-    MixBatch B;
-    B.n     = 1;
-    B.xs[0] = xs;
-    B.rs[0] = rs;
-    B.p[0]  = p;
-    B.v[0]  = v;
-    B.sc[0] = ctx->scalars;
-    return mix_update_batch<PB>(ctx, B);
-}
-
-template <int PB>
-int mix_p(c2q_ctx* ctx, c2q_spinor_eo* p, c2q_spinor_eo* rs)
-{
-    MixBatch B;
-    B.n     = 1;
-    B.rs[0] = rs;
-    B.p[0]  = p;
-    B.sc[0] = ctx->scalars;
-    return mix_p_batch<PB>(ctx, B);
-}
-
-int accumulate(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* xs)
+int accumulate(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* xs, const c2q_spinor_eo* p, const SolverScalars* sc)
 {
     const int n = x->geom.seo;
-    accumulate_kernel<32><<<(n + BLAS_THREADS - 1) / BLAS_THREADS, BLAS_THREADS, 0, ctx->stream>>>(
-        sptr<64>(x), sptr<32>(xs), n, x->geom.stride);
+    accumulate_kernel<PB><<<(n + BLAS_THREADS - 1) / BLAS_THREADS, BLAS_THREADS, 0, ctx->stream>>>(
+        sptr<64>(x), sptr<32>(xs), sptr<PB>(p), sc, n, x->geom.stride);
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
@@ -489,7 +467,11 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         t2[k] = &F.f[6 + 2 * n + 4 * k];
     }
     const int gk = gkind_for(PB, P->use_rec12 || PB == 16);
-    rc           = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
+    // FP64 true residuals on 12-real FP64 links when 12-real links were asked
+    // for (row 2 rebuilt in FP64: the operator agrees to rounding)
+    const int gk64 = P->use_rec12 ? G64R12 : G64;
+    rc             = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
+    if (!rc) rc = gauge_ensure(const_cast<c2q_gauge*>(g), gk64);
     if (rc) return rc;
     SolverScalars* dsc = nullptr;
     C2Q_CUDA(ctx, cudaMallocAsync(&dsc, n * sizeof(SolverScalars), ctx->stream));
@@ -532,7 +514,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
             rc   = launch_convert(ctx, rs[k], b[k]);
             s.r2 = s.b2;
         } else {
-            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps);
+            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, gk64);
             if (!rc) rc = launch_convert(ctx, rs[k], r64);
         }
         if (rc) return rc;
@@ -640,7 +622,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 s.status = C2Q_SOLVER_STUCK;
                 s.iters  = iter;
                 s.active = false;
-                rc       = accumulate(ctx, x[k], xs[k]);  // keep what was gained
+                rc       = accumulate<PB>(ctx, x[k], xs[k], p[k], nullptr);  // keep what was gained
                 if (rc) return rc;
                 continue;
             }
@@ -650,9 +632,9 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 // reliable update in FP64 after iteration `iter`
                 SolverScalars h;
                 rc = read_one(k, &h);
-                if (!rc) rc = accumulate(ctx, x[k], xs[k]);
+                if (!rc) rc = accumulate<PB>(ctx, x[k], xs[k], p[k], dsc + k);
                 if (!rc)
-                    rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps);
+                    rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, gk64);
                 if (rc) return rc;
                 ++s.reliable;
                 s.resid = s.r2;
@@ -672,6 +654,8 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 h.omega[0] = s.r2;
                 h.omega[1] = 0.0;
                 h.resid    = s.r2;
+                h.alpha[0] = 0.0;  // the deferred x update was accumulated
+                h.alpha[1] = 0.0;
                 rc         = write_one(k, h);
                 if (rc) return rc;
                 s.skip_upto = iter;
@@ -683,7 +667,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         if (S[k].active) {  // out of iterations: keep what was gained
             S[k].iters  = iter;
             S[k].active = false;
-            rc          = accumulate(ctx, x[k], xs[k]);
+            rc          = accumulate<PB>(ctx, x[k], xs[k], p[k], dsc + k);
             if (rc) return rc;
         }
     const double secs = clock.seconds();
@@ -692,7 +676,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         RhsState& s = S[k];
         double r2t  = s.r2_confirmed;
         if (r2t < 0) {
-            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &r2t, &s.sweeps);
+            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &r2t, &s.sweeps, gk64);
             if (rc) return rc;
         }
         finish_report(reps ? &reps[k] : nullptr, s.status, s.iters, s.reliable, s.resid,
@@ -906,7 +890,7 @@ C2Q_EXPORT void c2q_solver_params_default(c2q_solver_params* p)
     p->resid_check_every = 10;                   // :87
     p->min_iter          = 0;
     p->precision         = C2Q_PREC_FP64;
-    p->reliable_delta    = 0.01;
+    p->reliable_delta    = 0.003;
     p->use_rec12         = 0;
     p->use_graph         = 0;
 }

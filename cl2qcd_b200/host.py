@@ -387,7 +387,7 @@ class SolverParameters:
     resid_check_every: int = 10
     min_iter: int = 0
     precision: int = 64
-    reliable_delta: float = 0.01
+    reliable_delta: float = 0.003
     use_rec12: bool = False
     use_graph: bool = False
 

@@ -116,7 +116,7 @@ typedef struct {
     int resid_check_every;    /* solverResiduumCheckEvery (CG) */
     int min_iter;             /* solverMinIterations (CG) */
     int precision;            /* C2Q_PREC_*: inner arithmetic */
-    double reliable_delta;    /* mixed precision: reliable update when |r_inner| < delta * max|r| since the last one (default 0.01) */
+    double reliable_delta;    /* mixed precision: reliable update when |r_inner| < delta * max|r| since the last one (default 0.003) */
     int use_rec12;            /* inner operator uses 12-real links */
     int use_graph;            /* capture the iterations between residual checks in a CUDA graph */
 } c2q_solver_params;
