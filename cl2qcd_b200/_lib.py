@@ -45,6 +45,30 @@ class CSolveReport(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class CRequest(C.Structure):
+    _fields_ = [("lat", CLattice), ("gauge_id", C.c_ulonglong), ("kappa", C.c_double), ("mu", C.c_double),
+                ("nsrc", C.c_int), ("source_kind", C.c_int), ("source_seed", C.c_ulonglong),
+                ("params", CSolverParams), ("solutions", C.c_void_p)]
+
+
+class CRequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("nsrc", C.c_int), ("t_submit", C.c_double), ("t_admit", C.c_double),
+                ("t_done", C.c_double), ("iterations_max", C.c_int), ("true_resid_rel_max", C.c_double),
+                ("solution_norm2", C.c_double), ("footprint_bytes", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class CServerStats(C.Structure):
+    _fields_ = [("budget_bytes", C.c_longlong), ("gauge_bytes", C.c_longlong), ("reserved_bytes", C.c_longlong),
+                ("queued", C.c_int), ("running", C.c_int), ("slots", C.c_int), ("completed", C.c_longlong),
+                ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _P = C.c_void_p
 
@@ -104,6 +128,14 @@ SIGNATURES = {
                                            C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
     "c2q_gauge_generate": (C.c_int, [_D, C.c_int, C.c_int, C.c_double, C.c_ulonglong]),
     "c2q_source_generate": (C.c_int, [_D, C.c_size_t, C.c_int, C.c_ulonglong]),
+    "c2q_spinor_eo_source": (C.c_int, [_P, C.c_int, C.c_ulonglong]),
+    "c2q_server_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_int]),
+    "c2q_server_add_gauge": (C.c_int, [_P, C.c_ulonglong, C.POINTER(CLattice), _D]),
+    "c2q_server_submit": (C.c_int, [_P, C.POINTER(CRequest), C.POINTER(C.c_longlong)]),
+    "c2q_server_wait": (C.c_int, [_P, C.c_longlong, C.POINTER(CRequestResult)]),
+    "c2q_server_get_stats": (C.c_int, [_P, C.POINTER(CServerStats)]),
+    "c2q_server_destroy": (C.c_int, [_P]),
+    "c2q_request_footprint": (C.c_size_t, [C.POINTER(CLattice), C.c_int, C.c_int]),
 }
 
 _lib = None

@@ -978,6 +978,53 @@ C2Q_EXPORT int c2q_spinor_eo_zero(c2q_spinor_eo* f)
     return C2Q_OK;
 }
 
+// Seeded sources generated in place, site by site with the counter-based
+// SplitMix64 streams of c2q_source_generate (inputs.cpp): Z2 sources are
+// bit-identical to the host generator, Gaussian ones agree to the rounding of
+// the device's log / sqrt / sincos.
+__device__ __forceinline__ uint64_t smix_next(uint64_t& s)
+{
+    uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+    z          = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z          = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+__global__ void source_kernel(double2* f, int n, int stride, int kind, unsigned long long seed)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint64_t s = (seed ^ 0x5350494E4F52ULL) ^ ((uint64_t)i * 0x9E3779B97F4A7C15ULL + 0xD1B54A32D192ED03ULL);
+    smix_next(s);
+    if (kind == 0) {
+        const double h      = 1.0 / sqrt(2.0);  // as the host generator computes it
+        const uint64_t bits = smix_next(s);
+#pragma unroll
+        for (int k = 0; k < 12; ++k)
+            f[(size_t)k * stride + i] = make_double2(((bits >> (2 * k)) & 1) ? -h : h, ((bits >> (2 * k + 1)) & 1) ? -h : h);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const double u1 = ((smix_next(s) >> 11) + 1) * (1.0 / 9007199254740992.0);
+            const double u2 = ((smix_next(s) >> 11) + 1) * (1.0 / 9007199254740992.0);
+            const double r  = sqrt(-2.0 * log(u1));
+            double sn, cs;
+            sincos(6.283185307179586 * u2, &sn, &cs);
+            f[(size_t)k * stride + i] = make_double2(r * cs, r * sn);
+        }
+    }
+}
+
+C2Q_EXPORT int c2q_spinor_eo_source(c2q_spinor_eo* f, int kind, unsigned long long seed)
+{
+    if (!f || (kind != 0 && kind != 1)) return C2Q_BAD_ARG;
+    if (f->prec != 64) return fail(f->ctx, C2Q_BAD_ARG, "sources are generated into FP64 fields");
+    source_kernel<<<(f->geom.seo + 255) / 256, 256, 0, f->ctx->stream>>>((double2*)f->data, f->geom.seo,
+                                                                          f->geom.stride, kind, seed);
+    f->ctx->launches++;
+    C2Q_CUDA(f->ctx, cudaGetLastError());
+    return C2Q_OK;
+}
+
 // every component 1/sqrt(12 V) real (ocl_kernel/spinorfield_eo_cold.cl:22-33)
 __global__ void cold_kernel(double2* f, int n, int stride, double v)
 {

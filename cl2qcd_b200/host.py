@@ -494,3 +494,74 @@ def generate_source(n_sites: int, kind: str, seed: int) -> np.ndarray:
     out = np.zeros(n_sites * 24)
     _check(lib.c2q_source_generate(out, n_sites, {"z2": 0, "gaussian": 1}[kind], seed))
     return out.reshape(n_sites, 24)
+
+
+# ---------------- serving (no counterpart in the reference) ----------------
+class Server:
+    """Request loop on one GPU (c2q_server_*): `slots` worker threads with their
+    own streams; requests are admitted as soon as a slot and HBM (by
+    footprint) are free, so their work overlaps on the device; gauge fields are
+    registered once and stay resident.  Each request solves QplusQminus_eo for
+    `nsrc` seeded sources (generated on the device) with the multi-right-hand-
+    side mixed-precision CG."""
+
+    def __init__(self, device: int = 0, slots: int = 2, hbm_budget: int = 0, precision: int = 16,
+                 rec12: bool = True):
+        self.lib = L.load()
+        h = C.c_void_p()
+        _check(self.lib.c2q_server_create(C.byref(h), device, slots, hbm_budget, precision, int(rec12)))
+        self.h = h
+        self._keep = {}
+
+    def add_gauge(self, gauge_id: int, lattice: Lattice, aos: np.ndarray):
+        aos = np.ascontiguousarray(aos, dtype=np.float64).reshape(-1)
+        lc = lattice.c()
+        _check(self.lib.c2q_server_add_gauge(self.h, gauge_id, C.byref(lc), aos))
+
+    def submit(self, lattice: Lattice, gauge_id: int, kappa: float, mu: float, nsrc: int, seed: int,
+               source_kind: str = "z2", params: SolverParameters | None = None,
+               solutions: np.ndarray | None = None) -> int:
+        """Queue a request; `solutions` (optional, float64 (nsrc, Seo, 24)) receives the solutions."""
+        params = params or SolverParameters(solver="cg", prec=0.0, rel_tol=1e-10, cgmax=40000)
+        r = L.CRequest()
+        r.lat = lattice.c()
+        r.gauge_id = gauge_id
+        r.kappa, r.mu = kappa, mu
+        r.nsrc = nsrc
+        r.source_kind = {"z2": 0, "gaussian": 1}[source_kind]
+        r.source_seed = seed
+        r.params = params.c()
+        r.solutions = solutions.ctypes.data if solutions is not None else None
+        t = C.c_longlong()
+        _check(self.lib.c2q_server_submit(self.h, C.byref(r), C.byref(t)))
+        if solutions is not None:
+            self._keep[t.value] = solutions
+        return t.value
+
+    def wait(self, ticket: int) -> dict:
+        res = L.CRequestResult()
+        _check(self.lib.c2q_server_wait(self.h, ticket, C.byref(res)))
+        self._keep.pop(ticket, None)
+        return res.as_dict()
+
+    def stats(self) -> dict:
+        st = L.CServerStats()
+        _check(self.lib.c2q_server_get_stats(self.h, C.byref(st)))
+        return st.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.c2q_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def request_footprint(lattice: Lattice, nsrc: int, precision: int = 16) -> int:
+    """Device bytes a serving request holds while it runs (its admission footprint)."""
+    lc = lattice.c()
+    return L.load().c2q_request_footprint(C.byref(lc), nsrc, precision)

@@ -297,9 +297,61 @@ C2Q_EXPORT int c2q_gauge_generate(double* aos, int ns, int nt, double eps, unsig
 /* Seeded sources into host arrays of n_sites spinors:
  * kind 0 = Z2 noise ((+-1 +-i)/sqrt 2 per component), 1 = Gaussian (complex N(0,1) per component). */
 C2Q_EXPORT int c2q_source_generate(double* aos, size_t n_sites, int kind, unsigned long long seed);
+/* The same sources generated in place on the device into an FP64 eo field
+ * (Z2 bit-identical to c2q_source_generate; Gaussian equal to rounding). */
+C2Q_EXPORT int c2q_spinor_eo_source(c2q_spinor_eo* f, int kind, unsigned long long seed);
 
 /* Library version string. */
 C2Q_EXPORT const char* c2q_version(void);
+
+/* ---------------- serving (no counterpart in the reference) ----------------
+ * A request loop on one GPU.  The server owns `slots` worker threads, each with
+ * its own context and stream; queued requests are admitted, first fit in
+ * arrival order, as soon as a slot is free and their HBM footprint fits the
+ * budget, so their work overlaps on the device with the running requests.
+ * Gauge fields are registered once and stay resident.  Each request solves
+ * QplusQminus_eo x_k = b_k (twisted mass, mubar = 2 kappa mu) for nsrc seeded
+ * sources generated on the device, with the multi-right-hand-side mixed-
+ * precision CG at the server's inner precision and link format. */
+typedef struct c2q_server c2q_server;
+typedef struct {
+    c2q_lattice lat;                  /* must equal the registered gauge field's lattice */
+    unsigned long long gauge_id;
+    double kappa, mu;
+    int nsrc;                         /* 1..64 sources */
+    int source_kind;                  /* 0 Z2, 1 Gaussian (c2q_source_generate) */
+    unsigned long long source_seed;   /* source k uses seed + k */
+    c2q_solver_params params;         /* stopping test and limits; precision / use_rec12 come from the server */
+    double* solutions;                /* optional host array nsrc * Seo * 24 (eo AoS per source), or NULL */
+} c2q_request;
+typedef struct {
+    int status;                       /* C2Q_OK or the worst solver status; C2Q_OOM if it can never fit */
+    int nsrc;
+    double t_submit, t_admit, t_done; /* seconds since the server was created */
+    int iterations_max;
+    double true_resid_rel_max;        /* max over sources of ||b - A x|| / ||b|| in FP64 */
+    double solution_norm2;            /* sum over sources of |x|^2 (a checksum) */
+    long long footprint_bytes;
+} c2q_request_result;
+typedef struct {
+    long long budget_bytes, gauge_bytes, reserved_bytes;
+    int queued, running, slots;
+    long long completed;
+    double seconds;
+} c2q_server_stats;
+/* hbm_budget 0: 85% of the free device memory; precision 32 or 16 (inner CG). */
+C2Q_EXPORT int c2q_server_create(c2q_server** out, int device, int slots, size_t hbm_budget, int precision,
+                                 int rec12);
+C2Q_EXPORT int c2q_server_add_gauge(c2q_server* s, unsigned long long gauge_id, const c2q_lattice* lat,
+                                    const double* aos);
+C2Q_EXPORT int c2q_server_submit(c2q_server* s, const c2q_request* req, long long* ticket);
+/* Blocks until the request has finished (or failed); each ticket is waited on once. */
+C2Q_EXPORT int c2q_server_wait(c2q_server* s, long long ticket, c2q_request_result* out);
+C2Q_EXPORT int c2q_server_get_stats(c2q_server* s, c2q_server_stats* out);
+/* Finishes the running requests, cancels the queued ones (status C2Q_TIMEOUT). */
+C2Q_EXPORT int c2q_server_destroy(c2q_server* s);
+/* Device bytes one request holds while it runs (the admission footprint). */
+C2Q_EXPORT size_t c2q_request_footprint(const c2q_lattice* lat, int nsrc, int precision);
 
 #ifdef __cplusplus
 }

@@ -66,3 +66,16 @@ def test_source_generators(lib):
     assert np.allclose(np.abs(z), 1 / np.sqrt(2))
     gs = c2q.host.generate_source(20000, "gaussian", 3)
     assert abs(gs.mean()) < 0.02 and abs(gs.std() - 1) < 0.02
+
+
+def test_request_footprint_is_monotone():
+    """The serving admission footprint (host arithmetic only) grows with the
+    number of sources and the volume, and FP16 inner fields need less than FP32."""
+    import cl2qcd_b200 as c2q
+    small, big = c2q.Lattice(16, 32), c2q.Lattice(48, 96)
+    f = c2q.host.request_footprint
+    assert 0 < f(small, 1) < f(small, 2) < f(small, 12) < f(big, 1)
+    assert f(big, 12, 16) < f(big, 12, 32) <= f(big, 12, 64)
+    # 48^3x96 with 12 sources: about 53 GB, 32^3x64 with 12 about 10.5 GB
+    assert 50e9 < f(big, 12, 16) < 56e9
+    assert 10e9 < f(c2q.Lattice(32, 64), 12, 16) < 11e9
