@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=16, choices=[16, 32, 64])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving sweep only: Poisson requests at rising rates, p50/p99 latency and solves/s")
+    ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--serve-rates", default="0.5,1,2,4")
     ap.add_argument("--phase", default="all", choices=["all", "mixed"],
                     help="mixed: only the warm-up and timed mixed-precision solves (for profiling)")
     return ap.parse_args()
@@ -180,6 +184,62 @@ def cpu_reference_sample(g, b, fp64_iters, budget_s=15.0):
             "seconds_per_iteration": per_iter}
 
 
+SERVE_VOLUMES = [(16, 32), (24, 48), (32, 64), (48, 96)]
+
+
+def serving_run(c2q, rates, n_requests, slots=4, seed=4242, log=None):
+    """Poisson-arriving inversion requests: volume uniform over SERVE_VOLUMES
+    (one resident gauge field per volume, eps ~ U[0.2, 0.35]), kappa ~ U[0.14, 0.16],
+    mu ~ U[0.002, 0.02], 1-12 Z2 sources, mixed-precision (FP16 inner) to 1e-10.
+    For each arrival rate: latency = completion - submission per request,
+    p50 / p99 (nearest rank), and solves/s = sources solved / wall time."""
+    rng = np.random.default_rng(seed)
+    server = c2q.host.Server(0, slots=slots, precision=16)
+    lats = []
+    t_setup = time.time()
+    for v, (ns, nt) in enumerate(SERVE_VOLUMES):
+        lat = c2q.Lattice(ns, nt, 1.0, 0.0)
+        g = c2q.host.generate_gaugefield(lat, float(rng.uniform(0.2, 0.35)), 9000 + v)
+        server.add_gauge(v, lat, g)
+        del g
+        lats.append(lat)
+    t_setup = time.time() - t_setup
+    P = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000)
+    out = {"volumes": [f"{ns}^3x{nt}" for ns, nt in SERVE_VOLUMES], "slots": slots, "inner_precision": 16,
+           "sources": "Z2, 1-12 per request", "gauge_setup_s": round(t_setup, 1),
+           "budget_bytes": server.stats()["budget_bytes"], "gauge_bytes": server.stats()["gauge_bytes"],
+           "rates": []}
+    for rate in rates:
+        gaps = rng.exponential(1.0 / rate, n_requests)
+        reqs = [(int(rng.integers(0, len(SERVE_VOLUMES))), float(rng.uniform(0.14, 0.16)),
+                 float(rng.uniform(0.002, 0.02)), int(rng.integers(1, 13)), int(rng.integers(1, 1 << 40)))
+                for _ in range(n_requests)]
+        t0 = time.time()
+        tickets, next_t = [], 0.0
+        for gap, (v, kappa, mu, n, sd) in zip(gaps, reqs):
+            next_t += gap
+            dt = t0 + next_t - time.time()
+            if dt > 0:
+                time.sleep(dt)
+            tickets.append(server.submit(lats[v], v, kappa, mu, n, sd, params=P))
+        res = [server.wait(t) for t in tickets]
+        wall = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+        lat_s = sorted(r["t_done"] - r["t_submit"] for r in res)
+        q = lambda f: lat_s[min(len(lat_s) - 1, int(np.ceil(f * len(lat_s))) - 1)]
+        nsolved = sum(r["nsrc"] for r in res if r["status"] == 0)
+        entry = {"rate_per_s": rate, "requests": n_requests, "p50_s": round(q(0.5), 4), "p99_s": round(q(0.99), 4),
+                 "mean_s": round(float(np.mean(lat_s)), 4), "solves_per_s": round(nsolved / wall, 2),
+                 "requests_per_s": round(n_requests / wall, 3), "failed": sum(r["status"] != 0 for r in res),
+                 "true_resid_rel_max": max(r["true_resid_rel_max"] for r in res),
+                 "iterations_max": max(r["iterations_max"] for r in res),
+                 "queue_wait_mean_s": round(float(np.mean([r["t_admit"] - r["t_submit"] for r in res])), 4)}
+        out["rates"].append(entry)
+        if log:
+            log(entry)
+    server.close()
+    return out
+
+
 def inputs():
     import cl2qcd_b200 as c2q
     lat = c2q.Lattice(NS, NT, 1.0, 0.0)
@@ -220,6 +280,13 @@ def main():
 
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
+    if args.serve:
+        if rank == 0:
+            rates = [float(x) for x in args.serve_rates.split(",")]
+            res = serving_run(c2q, rates, args.serve_requests,
+                              log=lambda e: print(json.dumps({"serving_rate": e}), flush=True))
+            print(json.dumps({"metric": METRIC, "serving": res}))
+        return 0
     pg = None
     if ws > 1:
         import datetime
@@ -434,6 +501,8 @@ def main():
         return out
 
     mrhs = mrhs_section()
+    # serving stream at one arrival rate (the full sweep: --serve)
+    serving = serving_run(c2q, [1.0], args.serve_requests) if rank == 0 and ws == 1 else None
 
     cpu_baseline = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -478,6 +547,7 @@ def main():
             "speedup_mixed_vs_fp64": value / ws * fp64_s,
             "dslash_gbs": dg,
             "multi_rhs": mrhs,
+            "serving": serving,
             "autotune": system.tune_report().strip().splitlines(),
         }
         print(json.dumps(line))
