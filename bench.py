@@ -55,7 +55,7 @@ def parse():
                     help="serving sweep only: Poisson requests at rising rates, p50/p99 latency and solves/s")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rates", default="0.5,1,2,4")
-    ap.add_argument("--phase", default="all", choices=["all", "mixed"],
+    ap.add_argument("--phase", default="all", choices=["all", "mixed", "dslash"],
                     help="mixed: only the warm-up and timed mixed-precision solves (for profiling)")
     return ap.parse_args()
 
@@ -182,6 +182,37 @@ def cpu_reference_sample(g, b, fp64_iters, budget_s=15.0):
             "sample": f"{n} FP64 CG iterations (+1 refresh) of this 32^3x64 workload on the reference's kernels "
                       f"in {tn:.1f} s, scaled by {fp64_iters} FP64 iterations per solve",
             "seconds_per_iteration": per_iter}
+
+
+# algorithmic bytes per site of one plain dslash_eo sweep: 8 links + input + output
+DSLASH_BYTES = {(64, 0): 8 * 144 + 2 * 192, (64, 1): 8 * 96 + 2 * 192, (32, 0): 8 * 72 + 2 * 96,
+                (32, 1): 8 * 48 + 2 * 96, (16, 1): 8 * 24 + 2 * 52}
+
+
+def dslash_gbs(c2q, system, lat, gf, b, e0, e1, n=20):
+    """Achieved GB/s of c2q_dslash_eo (the public call) per storage precision and
+    link format, from CUDA events around n launches on the library's stream."""
+    import torch
+    lib = system.lib
+    out = {}
+    for (prec, rec12), per_site in DSLASH_BYTES.items():
+        system.set_link_format(rec12)
+        A_ = c2q.Spinorfield_eo(system, lat, b, precision=prec)
+        Y_ = c2q.Spinorfield_eo(system, lat, precision=prec)
+        for _ in range(3):
+            lib.c2q_dslash_eo(Y_.h, gf.h, A_.h, 1, KAPPA)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            lib.c2q_dslash_eo(Y_.h, gf.h, A_.h, 1, KAPPA)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3 / n
+        out[f"fp{prec}_{12 if rec12 else 18}real"] = {"gbs": round(lat.seo * per_site / sec / 1e9, 1),
+                                                     "us": round(sec * 1e6, 1), "bytes_per_site": per_site}
+        del A_, Y_
+    system.set_link_format(False)
+    return out
 
 
 SERVE_VOLUMES = [(16, 32), (24, 48), (32, 64), (48, 96)]
@@ -321,6 +352,12 @@ def main():
         c2q.host.cg(X, A, gf, B, P, add, rep)
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.phase == "dslash":
+        out = dslash_gbs(c2q, system, lat, gf, b, e0, e1)
+        if rank == 0:
+            print(json.dumps({"phase": "dslash", "dslash_gbs": out}))
+        system.close()
+        return 0
     if args.phase == "mixed":
         for _ in range(args.warmup):
             solve(P_mixed)
@@ -415,24 +452,7 @@ def main():
     if tr and str(args.precision) in tr.get("dram_bytes_per_launch", {}):
         traffic = tr["dram_bytes_per_launch"][str(args.precision)]
 
-    # ---- plain dslash bandwidth per precision (FP64 through the public call)
-    def dslash_gbs():
-        out = {}
-        Y = c2q.Spinorfield_eo(system, lat)
-        for _ in range(3):
-            lib.c2q_dslash_eo(Y.h, gf.h, B.h, 1, KAPPA)
-        torch.cuda.synchronize()
-        n = 20
-        e0.record()
-        for _ in range(n):
-            lib.c2q_dslash_eo(Y.h, gf.h, B.h, 1, KAPPA)
-        e1.record()
-        torch.cuda.synchronize()
-        sec = e0.elapsed_time(e1) / 1e3 / n
-        out["fp64_18real"] = round(lat.seo * 1536 / sec / 1e9, 1)
-        return out
-
-    dg = dslash_gbs()
+    dg = dslash_gbs(c2q, system, lat, gf, b, e0, e1)
 
     # ---- FP32-inner variant of the mixed solver, same problem (reported beside)
     P32 = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=32, use_rec12=True)
