@@ -55,7 +55,7 @@ def parse():
                     help="serving sweep only: Poisson requests at rising rates, p50/p99 latency and solves/s")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rates", default="0.5,1,2,4")
-    ap.add_argument("--phase", default="all", choices=["all", "mixed", "dslash"],
+    ap.add_argument("--phase", default="all", choices=["all", "mixed", "dslash", "large"],
                     help="mixed: only the warm-up and timed mixed-precision solves (for profiling)")
     return ap.parse_args()
 
@@ -215,6 +215,69 @@ def dslash_gbs(c2q, system, lat, gf, b, e0, e1, n=20):
     return out
 
 
+def large_volume(c2q, system, e0, e1):
+    """64^3x128 (16.8 M eo sites), eps 0.2, kappa 0.1625, mu 0.003, one Gaussian
+    source: dslash GB/s per precision (FP64 gauge 18-real vs 12-real) and the
+    solve time to a true residual 1e-10 of FP64 CG, FP64 BiCGStab (on Aee) and
+    mixed-precision CG (FP16 / FP32 inner)."""
+    import torch
+    ns, nt, kappa, mu = 64, 128, 0.1625, 0.003
+    lat = c2q.Lattice(ns, nt, 1.0, 0.0)
+    t = time.time()
+    g = c2q.host.generate_gaugefield(lat, 0.2, 64128)
+    gf = c2q.Gaugefield(system, lat, g)
+    del g
+    b = c2q.host.generate_source(lat.seo, "gaussian", 128)
+    setup_s = time.time() - t
+    out = {"lattice": "64^3x128", "eo_sites": lat.seo, "kappa": kappa, "mu": mu, "eps": 0.2,
+           "setup_s": round(setup_s, 1), "dslash_gbs": dslash_gbs(c2q, system, lat, gf, b, e0, e1, n=5)}
+    add = c2q.AdditionalParameters(kappa, 2 * kappa * mu)
+    B = c2q.Spinorfield_eo(system, lat, b)
+    X = c2q.Spinorfield_eo(system, lat)
+    b2 = float(np.vdot(b.reshape(-1), b.reshape(-1)))
+    runs = {
+        "fp64_cg": (c2q.host.cg, c2q.host.QplusQminus_eo(),
+                    c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=64)),
+        # the reference's BiCGStab "save" variant (true-residual recheck), bounded
+        "fp64_bicgstab_save": (c2q.host.bicgstab, c2q.host.Aee(),
+                               c2q.SolverParameters(solver="bicgstab_save", prec=REL_TOL ** 2 * b2, cgmax=2000)),
+        "mixed_fp16_cg": (c2q.host.cg, c2q.host.QplusQminus_eo(),
+                          c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=16,
+                                               use_rec12=True, use_graph=True)),
+        "mixed_fp32_cg": (c2q.host.cg, c2q.host.QplusQminus_eo(),
+                          c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=32,
+                                               use_rec12=True, use_graph=True)),
+    }
+    sols = {}
+    for name, (fn, A_, P_) in runs.items():
+        X.zero()
+        rep = {}
+        torch.cuda.synchronize()
+        e0.record()
+        try:
+            fn(X, A_, gf, B, P_, add, rep)
+            ok = True
+        except Exception as e:  # reported, not fatal
+            ok = repr(e)
+        e1.record()
+        torch.cuda.synchronize()
+        sec = e0.elapsed_time(e1) / 1e3
+        x = X.dump()
+        # true residual of the eo system the solver was given, in FP64 through the public operator
+        R = c2q.Spinorfield_eo(system, lat)
+        A_(R, gf, X, add)
+        r = R.dump() - b
+        out[name] = {"seconds": round(sec, 3), "iterations": rep.get("iterations"),
+                     "reliable_updates": rep.get("reliable_updates"), "ok": ok,
+                     "true_resid_rel": float(np.linalg.norm(r) / np.sqrt(b2))}
+        sols[name] = x
+        del R
+    ref = sols["fp64_cg"]
+    for name in ("mixed_fp16_cg", "mixed_fp32_cg"):
+        out[name]["rel_err_vs_fp64_cg"] = float(np.linalg.norm(sols[name] - ref) / np.linalg.norm(ref))
+    return out
+
+
 SERVE_VOLUMES = [(16, 32), (24, 48), (32, 64), (48, 96)]
 
 
@@ -352,6 +415,12 @@ def main():
         c2q.host.cg(X, A, gf, B, P, add, rep)
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.phase == "large":
+        out = large_volume(c2q, system, e0, e1)
+        if rank == 0:
+            print(json.dumps({"phase": "large", "large_volume": out}))
+        system.close()
+        return 0
     if args.phase == "dslash":
         out = dslash_gbs(c2q, system, lat, gf, b, e0, e1)
         if rank == 0:
