@@ -559,9 +559,9 @@ def main():
         t64 = e0.elapsed_time(e1) / 1e3
         out["fp64_single_rhs"] = {"solves_per_s": 12 / t64, "iterations": [r["iterations"] for r in reps64],
                                   "true_resid_rel_max": max(r["true_resid_rel"] for r in reps64)}
-        for prec in (32, 16):
+        for prec, rec12 in ((32, True), (16, True), (16, False)):
             Pm = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=prec,
-                                      use_rec12=True, use_graph=True)
+                                      use_rec12=rec12, use_graph=True)
             res = {}
             for n in (1, 4, 8, 12):
                 for x_ in Xs[:n]:
@@ -586,7 +586,7 @@ def main():
                                "reliable_updates": [r["reliable_updates"] for r in reps_],
                                "true_resid_rel_max": max(r["true_resid_rel"] for r in reps_),
                                "speedup_vs_fp64_single_rhs": (n / tb) / (12 / t64)}
-            out[f"fp{prec}_inner"] = res
+            out[f"fp{prec}_inner" + ("" if rec12 else "_18real_links")] = res
         return out
 
     mrhs = mrhs_section()

@@ -74,8 +74,9 @@ struct c2q_gauge {
     c2q_ctx* ctx = nullptr;
     c2q_lattice lat{};
     c2q::Geom geom{};
-    // [0] FP64 18-real, [1] FP64 12-real, [2] FP32 18-real, [3] FP32 12-real, [4] FP16 12-real
-    c2q::GaugeStore store[5];
+    // [0] FP64 18-real, [1] FP64 12-real, [2] FP32 18-real, [3] FP32 12-real, [4] FP16 12-real,
+    // [5] FP16 18-real
+    c2q::GaugeStore store[6];
 };
 
 struct c2q_spinor_eo {
@@ -90,7 +91,7 @@ struct c2q_spinor_eo {
 
 namespace c2q {
 
-enum GaugeKind { G64 = 0, G64R12 = 1, G32 = 2, G32R12 = 3, G16R12 = 4 };
+enum GaugeKind { G64 = 0, G64R12 = 1, G32 = 2, G32R12 = 3, G16R12 = 4, G16 = 5 };
 
 // ---- status plumbing ----
 int fail(c2q_ctx* ctx, int code, const std::string& msg);

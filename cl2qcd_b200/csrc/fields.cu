@@ -147,7 +147,7 @@ int gkind_for(int prec, int rec12)
 {
     if (prec == 64) return rec12 ? G64R12 : G64;
     if (prec == 32) return rec12 ? G32R12 : G32;
-    return G16R12;
+    return rec12 ? G16R12 : G16;
 }
 
 cudaEvent_t profile_event(c2q_ctx* ctx)
@@ -278,9 +278,11 @@ __global__ void gauge_convert32_kernel(const double2* __restrict__ in, float4* _
     }
 }
 
-// FP64 9-lane store -> FP16 12-real slot layout: rows 0 and 1 as biased
-// 16-bit fixed point (u = rint(v * 32767) + 32768, v clamped to [-1, 1]),
-// three uint4 lanes (entry 2L of both sites, entry 2L+1 of both sites).
+// FP64 9-lane store -> FP16 slot layout, biased 16-bit fixed point
+// (u = rint(v * 32767) + 32768, v clamped to [-1, 1]).  12-real (NL = 6):
+// rows 0 and 1 as three uint4 lanes (entry 2L of both sites, entry 2L+1 of both
+// sites); 18-real (NL = 9): entries 0..7 as four uint4 lanes, entry 8 of both
+// sites as one uint2 lane after them.
 __device__ __forceinline__ unsigned enc16(double2 v)
 {
     const double cx = fmin(1.0, fmax(-1.0, v.x)), cy = fmin(1.0, fmax(-1.0, v.y));
@@ -288,6 +290,7 @@ __device__ __forceinline__ unsigned enc16(double2 v)
     const int hi    = __double2int_rn(cy * 32767.0) + 32768;
     return (unsigned)(lo & 0xffff) | ((unsigned)hi << 16);
 }
+template <int NL>
 __global__ void gauge_convert16_kernel(const double2* __restrict__ in, uint4* __restrict__ out, Geom g)
 {
     const int ss = g.stride / 2, H = g.seo / 2;
@@ -296,12 +299,19 @@ __global__ void gauge_convert16_kernel(const double2* __restrict__ in, uint4* __
     const int blk = (int)(t / ss), j = (int)(t - (long long)blk * ss);
     if (j >= H) return;
     const double2* src = in + (size_t)blk * 9 * g.stride;
-    uint4* dst         = out + (size_t)blk * 3 * ss + j;
+    // a (parity, mu) group: 48 (12-real) or 72 (18-real) bytes per slot
+    char* grp   = reinterpret_cast<char*>(out) + (size_t)blk * (NL == 6 ? 48 : 72) * ss;
+    uint4* dst  = reinterpret_cast<uint4*>(grp) + j;
+    constexpr int LANES = NL == 6 ? 3 : 4;
 #pragma unroll
-    for (int L = 0; L < 3; ++L) {
+    for (int L = 0; L < LANES; ++L) {
         const size_t e0 = (size_t)(2 * L) * g.stride, e1 = (size_t)(2 * L + 1) * g.stride;
         dst[(size_t)L * ss] = make_uint4(enc16(src[e0 + j]), enc16(src[e0 + j + H]), enc16(src[e1 + j]),
                                          enc16(src[e1 + j + H]));
+    }
+    if (NL == 9) {
+        uint2* tail = reinterpret_cast<uint2*>(grp + (size_t)64 * ss) + j;
+        *tail       = make_uint2(enc16(src[(size_t)8 * g.stride + j]), enc16(src[(size_t)8 * g.stride + j + H]));
     }
 }
 
@@ -317,6 +327,7 @@ int gauge_ensure(c2q_gauge* g, int kind)
         case G32: bytes = lanes * 9 * 8; break;
         case G32R12: bytes = lanes * 6 * 8; break;
         case G16R12: bytes = lanes * 6 * 4; break;
+        case G16: bytes = lanes * 9 * 4; break;
         default: return fail(ctx, C2Q_BAD_ARG, "bad gauge kind");
     }
     void* p = nullptr;
@@ -332,7 +343,8 @@ int gauge_ensure(c2q_gauge* g, int kind)
         case G64R12: gauge_convert64_kernel<<<blocks, threads, 0, ctx->stream>>>(src, (double2*)p, g->geom); break;
         case G32: gauge_convert32_kernel<9><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
         case G32R12: gauge_convert32_kernel<6><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
-        case G16R12: gauge_convert16_kernel<<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
+        case G16R12: gauge_convert16_kernel<6><<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
+        case G16: gauge_convert16_kernel<9><<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
     }
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
@@ -392,7 +404,7 @@ static int dslash_typed(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_
         if (rc) return rc;
     }
     prm.red = red_args(ctx, dot.fin);
-    const bool r12 = gkind == G64R12 || gkind == G32R12 || gkind == G16R12;
+    const bool r12 = gkind == G64R12 || gkind == G32R12 || gkind == G16R12;  // FP64 here
     c2q_ctx::Timed tm{};
     if (ctx->profiling) {
         tm.a     = profile_event(ctx);
@@ -424,7 +436,7 @@ static bool gauge_matches(int prec, int gkind)
 {
     if (prec == 64) return gkind == G64 || gkind == G64R12;
     if (prec == 32) return gkind == G32 || gkind == G32R12;
-    return gkind == G16R12;
+    return gkind == G16R12 || gkind == G16;
 }
 
 int launch_dslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_eo* out, const c2q_spinor_eo* in,

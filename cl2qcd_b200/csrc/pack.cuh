@@ -22,7 +22,9 @@
 //                w[2L+1] site 1) with w[c] = re | im << 16 in the biased 16-bit
 //                fixed point of c2q_internal.cuh; per-site norms as float2;
 //   FP32 links : NL lanes (9 or 6 complex entries) of float4 per (parity, mu);
-//   FP16 links : rows 0 and 1 (6 entries) as 3 lanes of uint4 per (parity, mu).
+//   FP16 links : 12-real: rows 0 and 1 (6 entries) as 3 lanes of uint4 per
+//                (parity, mu); 18-real: entries 0..7 as 4 uint4 lanes and entry 8
+//                as one uint2 lane.
 // Lane stride = `ss` slots (half the FP64 lane stride, a multiple of 32).
 #pragma once
 
@@ -165,32 +167,6 @@ struct SlotF16 {
     }
 };
 
-// Generic slot access by storage precision (P = 32 or 16).
-template <int P>
-struct SlotIO;
-template <>
-struct SlotIO<32> {
-    static __device__ __forceinline__ void load(const SpinorPtr<32>& f, int ss, int j, C2 s[12])
-    {
-        SlotF32::load(f.data, ss, j, s);
-    }
-    static __device__ __forceinline__ void store(const SpinorPtr<32>& f, int ss, int j, const C2 s[12])
-    {
-        SlotF32::store(f.data, ss, j, s);
-    }
-};
-template <>
-struct SlotIO<16> {
-    static __device__ __forceinline__ void load(const SpinorPtr<16>& f, int ss, int j, C2 s[12])
-    {
-        SlotF16::load(f.data, f.norm, ss, j, s);
-    }
-    static __device__ __forceinline__ void store(const SpinorPtr<16>& f, int ss, int j, const C2 s[12])
-    {
-        SlotF16::store(f.data, f.norm, ss, j, s);
-    }
-};
-
 // ------------------------------------------------------------------ links
 // row2 = s * conj(row0 x row1) on slot pairs; (a x b)_k = a_{k+1} b_{k+2} - a_{k+2} b_{k+1}
 __device__ __forceinline__ void cross_conj(C2& out, C2 a, C2 b, C2 c, C2 d, float s)
@@ -209,42 +185,5 @@ __device__ __forceinline__ void reconstruct_row2_pk(C2 u[9], float s)
     cross_conj(u[7], u[2], u[3], u[0], u[5], s);
     cross_conj(u[8], u[0], u[4], u[1], u[3], s);
 }
-
-template <int P, int NL>
-struct SlotLink;
-
-// FP32 links, NL = 9 (18-real) or 6 (12-real)
-template <int NL>
-struct SlotLink<32, NL> {
-    template <bool SWP>
-    static __device__ __forceinline__ void load(const void* base, size_t ls, size_t j, C2 u[9])
-    {
-        const float4* p = static_cast<const float4*>(base);
-#pragma unroll
-        for (int e = 0; e < NL; ++e) u[e] = c2_from(__ldg(p + e * ls + j), SWP);
-        if (NL == 6) reconstruct_row2_pk(u, 1.0f);
-    }
-};
-
-// FP16 links (12-real, fixed scale 1/32767): entries returned in units of 1/32767
-template <int NL>
-struct SlotLink<16, NL> {
-    static_assert(NL == 6, "FP16 links are stored 12-real");
-    template <bool SWP>
-    static __device__ __forceinline__ void load(const void* base, size_t ls, size_t j, C2 u[9])
-    {
-        const uint4* p   = static_cast<const uint4*>(base);
-        const float2 nb  = bc2(-FIX_BIAS);
-#pragma unroll
-        for (int L = 0; L < 3; ++L) {
-            const uint4 v   = __ldg(p + L * ls + j);
-            const uint2 wa  = SWP ? make_uint2(v.y, v.x) : make_uint2(v.x, v.y);
-            const uint2 wb  = SWP ? make_uint2(v.w, v.z) : make_uint2(v.z, v.w);
-            u[2 * L]        = C2{add2(blo(wa), nb), add2(bhi(wa), nb)};
-            u[2 * L + 1]    = C2{add2(blo(wb), nb), add2(bhi(wb), nb)};
-        }
-        reconstruct_row2_pk(u, 1.0f / 32767.0f);
-    }
-};
 
 }  // namespace c2q

@@ -11,8 +11,8 @@ namespace c2q {
 
 void pk_dispatch32_c0(const PkParams<32>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
 void pk_dispatch32_c1(const PkParams<32>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
-void pk_dispatch16_c0(const PkParams<16>& prm, int epi, int dot, int blocks, cudaStream_t s);
-void pk_dispatch16_c1(const PkParams<16>& prm, int epi, int dot, int blocks, cudaStream_t s);
+void pk_dispatch16_c0(const PkParams<16>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
+void pk_dispatch16_c1(const PkParams<16>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
 
 // Resident blocks per SM of a configuration: its launch bound, or what its
 // shared-memory ring leaves room for (228 KB per SM, 1 KB reserved per block).
@@ -20,9 +20,12 @@ static int pk_blocks_per_sm(int P, int nl, int cfg)
 {
     int minb     = 0;
     size_t bytes = 0;
-    if (P == 16) {
+    if (P == 16 && nl == 6) {
         minb  = cfg ? PkStage<16, 6, 1>::MINB : PkStage<16, 6, 0>::MINB;
         bytes = cfg ? PkStage<16, 6, 1>::BYTES : PkStage<16, 6, 0>::BYTES;
+    } else if (P == 16) {
+        minb  = cfg ? PkStage<16, 9, 1>::MINB : PkStage<16, 9, 0>::MINB;
+        bytes = cfg ? PkStage<16, 9, 1>::BYTES : PkStage<16, 9, 0>::BYTES;
     } else if (nl == 6) {
         minb  = cfg ? PkStage<32, 6, 1>::MINB : PkStage<32, 6, 0>::MINB;
         bytes = cfg ? PkStage<32, 6, 1>::BYTES : PkStage<32, 6, 0>::BYTES;
@@ -56,9 +59,9 @@ static void pk_dispatch(const PkParams<P>& prm, int cfg, int nl, int epi, int do
 {
     if constexpr (P == 16) {
         if (cfg)
-            pk_dispatch16_c1(prm, epi, dot, blocks, s);
+            pk_dispatch16_c1(prm, nl, epi, dot, blocks, s);
         else
-            pk_dispatch16_c0(prm, epi, dot, blocks, s);
+            pk_dispatch16_c0(prm, nl, epi, dot, blocks, s);
     } else {
         if (cfg)
             pk_dispatch32_c1(prm, nl, epi, dot, blocks, s);
@@ -183,7 +186,7 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     prm.red.result   = ctx->red_result;
     prm.red.sc       = ctx->scalars;
     prm.red.fin      = B.fin;
-    const bool r12   = gkind == G32R12 || gkind == G16R12;
+    const bool r12   = gkind == G32R12 || gkind == G16R12;  // else 18-real
     const int nl     = r12 ? 6 : 9;
     int choice       = 0;
     int rc           = pk_choose<P>(ctx, prm, nl, B.epi, B.dot_mode, &choice);

@@ -188,7 +188,8 @@ constexpr int PK_CONFIGS = 2;
 template <int P, int NL>
 struct PkChunks {
     static constexpr int SPC = P == 16 ? 7 : 12;
-    static constexpr int LKC = P == 16 ? 3 : NL;
+    // FP16 18-real: entries 0..7 in four chunks, entry 8 in half of a fifth
+    static constexpr int LKC = P == 16 ? (NL == 6 ? 3 : 5) : NL;
     static constexpr int CH  = SPC + LKC;
 };
 template <int P, int NL, int CFG>
@@ -231,8 +232,14 @@ __device__ __forceinline__ void stage_link(uint4* st, const char* links, int ss,
 {
     constexpr int SPC = PkChunks<P, NL>::SPC, LKC = PkChunks<P, NL>::LKC;
     const uint4* p    = reinterpret_cast<const uint4*>(links) + slot;
+    if constexpr (P == 16 && NL == 9) {
 #pragma unroll
-    for (int c = 0; c < LKC; ++c) cp16(st + (SPC + c) * PK_THREADS, p + (size_t)c * ss);
+        for (int c = 0; c < 4; ++c) cp16(st + (SPC + c) * PK_THREADS, p + (size_t)c * ss);
+        cp8(st + (SPC + 4) * PK_THREADS, reinterpret_cast<const uint2*>(links + (size_t)64 * ss) + slot);
+    } else {
+#pragma unroll
+        for (int c = 0; c < LKC; ++c) cp16(st + (SPC + c) * PK_THREADS, p + (size_t)c * ss);
+    }
 }
 
 __device__ __forceinline__ float4 as_f4(uint4 v)
@@ -246,15 +253,22 @@ __device__ __forceinline__ void staged_link(const uint4* lk, C2 u[9])
 {
     if constexpr (P == 16) {
         const float2 nb = bc2(-FIX_BIAS);
+        constexpr int L2 = NL == 6 ? 3 : 4;
 #pragma unroll
-        for (int L = 0; L < 3; ++L) {
+        for (int L = 0; L < L2; ++L) {
             const uint4 v  = lk[L * PK_THREADS];
             const uint2 wa = SWP ? make_uint2(v.y, v.x) : make_uint2(v.x, v.y);
             const uint2 wb = SWP ? make_uint2(v.w, v.z) : make_uint2(v.z, v.w);
             u[2 * L]       = C2{add2(blo(wa), nb), add2(bhi(wa), nb)};
             u[2 * L + 1]   = C2{add2(blo(wb), nb), add2(bhi(wb), nb)};
         }
-        reconstruct_row2_pk(u, 1.0f / 32767.0f);
+        if constexpr (NL == 9) {
+            const uint4 v  = lk[4 * PK_THREADS];
+            const uint2 wa = SWP ? make_uint2(v.y, v.x) : make_uint2(v.x, v.y);
+            u[8]           = C2{add2(blo(wa), nb), add2(bhi(wa), nb)};
+        } else {
+            reconstruct_row2_pk(u, 1.0f / 32767.0f);
+        }
     } else {
 #pragma unroll
         for (int e = 0; e < NL; ++e) u[e] = c2_from(as_f4(lk[e * PK_THREADS]), SWP);
@@ -362,11 +376,11 @@ __device__ __forceinline__ void pk_hop_ph(C2 acc[12], const PkParams<P>& prm, co
     }
 }
 
-// 16-byte lanes per (parity, mu) group of links in the slot layout
+// bytes per slot of a (parity, mu) group of links in the slot layout
 template <int P, int NL>
-__host__ __device__ constexpr int pk_link_lanes()
+__host__ __device__ constexpr int pk_link_bytes()
 {
-    return P == 16 ? 3 : NL;
+    return P == 16 ? (NL == 6 ? 48 : 72) : 16 * NL;
 }
 
 template <int P, int NL, int EPI, int DOT, int PH, int CFG>
@@ -403,8 +417,7 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
         const int ss      = g.ss;
 
         const int po          = prm.out_parity;
-        constexpr int LL      = pk_link_lanes<P, NL>();
-        const size_t grp      = (size_t)LL * ss * 16;
+        const size_t grp      = (size_t)pk_link_bytes<P, NL>() * ss;
         const char* gb        = static_cast<const char*>(prm.gauge);
         const char* fwd_links = gb + (size_t)(po * 4) * grp;
         const char* bwd_links = gb + (size_t)((1 - po) * 4) * grp;

@@ -248,7 +248,7 @@ C2Q_EXPORT int c2q_server_add_gauge(c2q_server* s, unsigned long long gauge_id, 
     if (!rc) rc = c2q_gauge_upload(g, aos);
     // every storage the server's solvers read, built now so that the slots
     // only ever read the gauge object
-    const int inner = s->precision == 16 ? G16R12 : (s->rec12 ? G32R12 : G32);
+    const int inner = gkind_for(s->precision, s->rec12);
     if (!rc) rc = gauge_ensure(g, inner);
     if (!rc && s->rec12) rc = gauge_ensure(g, G64R12);
     if (!rc) rc = c2q_ctx_synchronize(s->loader);

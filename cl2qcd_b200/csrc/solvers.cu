@@ -466,7 +466,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         t1[k] = &F.f[5 + 2 * n + 4 * k];
         t2[k] = &F.f[6 + 2 * n + 4 * k];
     }
-    const int gk = gkind_for(PB, P->use_rec12 || PB == 16);
+    const int gk = gkind_for(PB, P->use_rec12);
     // FP64 true residuals on 12-real FP64 links when 12-real links were asked
     // for (row 2 rebuilt in FP64: the operator agrees to rounding)
     const int gk64 = P->use_rec12 ? G64R12 : G64;

@@ -90,7 +90,7 @@ RP_LATTICES = [(4, 4, 0.0, 0.0, None, None), (8, 8, 1.0, 0.0, None, None), (6, 8
 
 
 @pytest.mark.parametrize("lat", RP_LATTICES)
-@pytest.mark.parametrize("precision,rec12", [(32, False), (32, True), (16, True)])
+@pytest.mark.parametrize("precision,rec12", [(32, False), (32, True), (16, True), (16, False)])
 def test_reduced_precision_operators_match_oracle(port, system, O, lat, precision, rec12):
     """The FP32 / FP16 paired-site sweeps against the FP64 oracle: the dslash on
     both parities, the fused dslash + M_tm^{-1}, and Q+Q- (all four fused sweep
