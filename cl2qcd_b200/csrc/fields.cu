@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 
 #include "blas.cuh"
 #include "c2q_host.h"
@@ -1034,6 +1035,66 @@ C2Q_EXPORT int c2q_spinor_eo_source(c2q_spinor_eo* f, int kind, unsigned long lo
                                                                           f->geom.stride, kind, seed);
     f->ctx->launches++;
     C2Q_CUDA(f->ctx, cudaGetLastError());
+    return C2Q_OK;
+}
+
+// Pseudoscalar correlator from point sources in the time direction
+// (ocl_kernel/fermionobservables/correlator_ps_point.cl, correlator_ps_t):
+// C(t) = (2 kappa)^2 / NS^3 * sum over the solutions and the sites of time
+// slice t of |phi|^2.  The eo index runs with t slowest, so slice t of each
+// parity is the contiguous range [t NS^3/2, (t+1) NS^3/2).  One block per time
+// slice sums in a fixed order: deterministic.
+constexpr int CORR_THREADS = 256;
+__global__ void correlator_ps_t_kernel(const double2* const* fields, int nfields, int per_slice, int stride,
+                                       double factor, double* out)
+{
+    const int t = blockIdx.x;
+    double acc[1] = {0.0};
+    for (int f = 0; f < nfields; ++f) {
+        const double2* p = fields[f];
+        for (int i = threadIdx.x; i < per_slice; i += blockDim.x) {
+            const int site = t * per_slice + i;
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                const double2 v = p[(size_t)k * stride + site];
+                acc[0] += v.x * v.x + v.y * v.y;
+            }
+        }
+    }
+    __shared__ double smem[32];
+    block_sum<1>(acc, smem);
+    if (threadIdx.x == 0) out[t] = factor * acc[0];
+}
+
+C2Q_EXPORT int c2q_correlator_ps(const c2q_spinor_eo* const* even, const c2q_spinor_eo* const* odd, int n,
+                                 double kappa, double* out)
+{
+    if (!even || !odd || n < 1 || !out || !even[0]) return C2Q_BAD_ARG;
+    c2q_ctx* ctx = even[0]->ctx;
+    const Geom& g = even[0]->geom;
+    std::vector<const double2*> ptrs;
+    for (int k = 0; k < n; ++k) {
+        for (const c2q_spinor_eo* f : {even[k], odd[k]}) {
+            if (!f || f->prec != 64 || f->ctx != ctx || !same_lattice(f->lat, even[0]->lat))
+                return fail(ctx, C2Q_BAD_ARG, "correlator fields must be FP64 fields of one context and lattice");
+            ptrs.push_back(static_cast<const double2*>(f->data));
+        }
+    }
+    const size_t pbytes = ptrs.size() * sizeof(void*);
+    const size_t obytes = (size_t)g.nt * sizeof(double);
+    int rc              = ensure_staging(ctx, pbytes + obytes);
+    if (rc) return rc;
+    char* stage = static_cast<char*>(ctx->staging);
+    C2Q_CUDA(ctx, cudaMemcpyAsync(stage, ptrs.data(), pbytes, cudaMemcpyHostToDevice, ctx->stream));
+    // the pointer array is read by the kernel before the host vector goes away
+    const double factor = 2.0 * kappa * 2.0 * kappa / ((double)g.ns * g.ns * g.ns);
+    double* dout        = reinterpret_cast<double*>(stage + ((pbytes + 15) / 16) * 16);
+    correlator_ps_t_kernel<<<g.nt, CORR_THREADS, 0, ctx->stream>>>(
+        reinterpret_cast<const double2* const*>(stage), (int)ptrs.size(), g.vs_h, g.stride, factor, dout);
+    ctx->launches++;
+    C2Q_CUDA(ctx, cudaGetLastError());
+    C2Q_CUDA(ctx, cudaMemcpyAsync(out, dout, obytes, cudaMemcpyDeviceToHost, ctx->stream));
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return C2Q_OK;
 }
 

@@ -965,6 +965,23 @@ C2Q_EXPORT int c2q_perform_inversion_eo(c2q_ctx* ctx, double* result, const c2q_
 {
     if (!ctx || !result || !g || !source || !p) return C2Q_BAD_ARG;
     Fields F;
+    int rc = make_fields(ctx, g->lat, 64, 2, F, 0);
+    if (rc) return rc;
+    const int conv = c2q_perform_inversion_eo_fields(ctx, &F.f[0], &F.f[1], g, source, kappa, mubar, action, p, report);
+    if (conv < 0) return conv;
+    rc = c2q_convert_from_eoprec(result, &F.f[0], &F.f[1]);
+    return rc ? rc : conv;
+}
+
+C2Q_EXPORT int c2q_perform_inversion_eo_fields(c2q_ctx* ctx, c2q_spinor_eo* out_even, c2q_spinor_eo* out_odd,
+                                               const c2q_gauge* g, const double* source, double kappa, double mubar,
+                                               int action, const c2q_solver_params* p, c2q_solve_report* report)
+{
+    if (!ctx || !out_even || !out_odd || !g || !source || !p) return C2Q_BAD_ARG;
+    if (out_even->prec != 64 || out_odd->prec != 64 || !same_lattice(out_even->lat, g->lat) ||
+        !same_lattice(out_odd->lat, g->lat))
+        return fail(ctx, C2Q_BAD_ARG, "inversion results must be FP64 fields on the gauge field's lattice");
+    Fields F;
     int rc = make_fields(ctx, g->lat, 64, 5, F, 0);
     if (rc) return rc;
     c2q_spinor_eo *src_even = &F.f[0], *src_odd = &F.f[1], *tmp1 = &F.f[2], *tmp2 = &F.f[3], *res = &F.f[4];
@@ -1011,7 +1028,9 @@ C2Q_EXPORT int c2q_perform_inversion_eo(c2q_ctx* ctx, double* result, const c2q_
         if (!rc) rc = c2q_sax(tmp1, -1, 0, tmp1);
     }
     if (rc) return rc;
-    rc = c2q_convert_from_eoprec(result, tmp1, res);
+    // the even sites of the full result are tmp1, the odd ones res (parity roles swapped back)
+    rc = c2q_copyData(out_even, tmp1);
+    if (!rc) rc = c2q_copyData(out_odd, res);
     return rc ? rc : conv;
 }
 

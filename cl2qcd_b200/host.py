@@ -480,6 +480,47 @@ def perform_inversion(system: System, gf: Gaugefield, source: np.ndarray, params
     return out.reshape(gf.lattice.vol, 24), rc
 
 
+def point_source_full(lattice: Lattice, k: int, x: int = 0, y: int = 0, z: int = 0, t: int = 0) -> np.ndarray:
+    """Full-field point source k (spin k % 4, colour k // 4, content "one") at
+    (x, y, z, t) (spinorfield_point_source.cl:23-75, physics/sources.cpp:35-60)."""
+    out = np.zeros((lattice.vol, 24))
+    site = x + lattice.ns * (y + lattice.ns * (z + lattice.ns * t))
+    out[site, 2 * (3 * (k % 4) + k // 4)] = 1.0
+    return out
+
+
+def inverter_ps_correlator(system: System, gf: Gaugefield, params: SolverParameters, add: AdditionalParameters,
+                           n_sources: int = 12, position=(0, 0, 0, 0), action: str = "twistedmass",
+                           reports: list | None = None) -> np.ndarray:
+    """The inverter's point-source measurement (physics/observables/wilsonTwoFlavourCorrelators.cpp:
+    measureTwoFlavourDoubletCorrelatorsOnGaugefieldAndWriteToFile with the default 12 point
+    sources): perform_inversion (eo) of each spin-colour point source, results kept on the
+    device, and the pseudoscalar correlator C(t) contracted on the GPU."""
+    lib = system.lib
+    L_ = gf.lattice
+    act = L.WILSON if action.lower() == "wilson" else L.TWISTEDMASS
+    evens = [Spinorfield_eo(system, L_) for _ in range(n_sources)]
+    odds = [Spinorfield_eo(system, L_) for _ in range(n_sources)]
+    p = params.c()
+    for k in range(n_sources):
+        src = point_source_full(L_, k % 12, *position).reshape(-1)
+        rep = L.CSolveReport()
+        rc = lib.c2q_perform_inversion_eo_fields(system.h, evens[k].h, odds[k].h, gf.h, src, add.kappa, add.mubar,
+                                                 act, C.byref(p), C.byref(rep))
+        if reports is not None:
+            reports.append(rep.as_dict())
+        if rc == L.SOLVER_STUCK:
+            raise SolverStuck(rep.iterations)
+        if rc == L.DID_NOT_SOLVE:
+            raise SolverDidNotSolve(rep.iterations)
+        _check(rc, system.h, lib)
+    out = np.zeros(L_.nt)
+    ae = (C.c_void_p * n_sources)(*[f.h for f in evens])
+    ao = (C.c_void_p * n_sources)(*[f.h for f in odds])
+    _check(lib.c2q_correlator_ps(ae, ao, n_sources, add.kappa, out), system.h, lib)
+    return out
+
+
 # ---------------- inputs ----------------
 def generate_gaugefield(lattice: Lattice, eps: float, seed: int) -> np.ndarray:
     """U = exp(i eps H), reunitarised (host, library code)."""

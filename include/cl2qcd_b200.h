@@ -288,6 +288,18 @@ C2Q_EXPORT int c2q_cg_multi(c2q_spinor_eo* const* x, int op, const c2q_gauge* g,
 C2Q_EXPORT int c2q_perform_inversion_eo(c2q_ctx* ctx, double* result, const c2q_gauge* g, const double* source,
                                         double kappa, double mubar, int action, const c2q_solver_params* p,
                                         c2q_solve_report* report);
+/* The same inversion with the result left on the device: out_even / out_odd
+ * receive the sites with x+y+z+t even / odd of the full result (FP64 fields). */
+C2Q_EXPORT int c2q_perform_inversion_eo_fields(c2q_ctx* ctx, c2q_spinor_eo* out_even, c2q_spinor_eo* out_odd,
+                                               const c2q_gauge* g, const double* source, double kappa, double mubar,
+                                               int action, const c2q_solver_params* p, c2q_solve_report* report);
+/* Pseudoscalar correlator from point sources in the time direction
+ * (physics/observables/wilsonTwoFlavourCorrelators.cpp:162-415 with
+ * ocl_kernel/fermionobservables/correlator_ps_point.cl correlator_ps_t):
+ * out[t] = (2 kappa)^2 / NS^3 * sum_k sum_{x in slice t} |phi_k(x)|^2 over the n
+ * full solutions phi_k = (even[k], odd[k]); out is a host array of NT doubles. */
+C2Q_EXPORT int c2q_correlator_ps(const c2q_spinor_eo* const* even, const c2q_spinor_eo* const* odd, int n,
+                                 double kappa, double* out);
 
 /* ---------------- inputs ---------------- */
 /* Seeded synthetic gauge field U = exp(i eps H), H traceless Hermitian with

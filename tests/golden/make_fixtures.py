@@ -80,6 +80,18 @@ def extract_kats(ref: str) -> dict:
     out["tm_sitediagonal_per_site"] = {"values": diag, "kappa": 0.123456, "mu": 0.123456,
                                        "fill": "ascendingComplex", "lattice": [4, 8],
                                        "where": "hardware/code/fermions_test.cpp:69-104,483-507"}
+    # integration references of the inverter executable (executables/tests/testInverter.py:
+    # the pseudoscalar correlator lines, compared at 0.1 %), with their input files
+    out["inverter"] = {}
+    for name, inp in (("inverter_test_ref", "inverter_test_input_1"), ("inverter_test_ref2", "inverter_test_input_2")):
+        vals = _floats(open(os.path.join(ref, "executables/tests", name)).read())
+        params = {}
+        for line in open(os.path.join(ref, "executables/tests", inp)):
+            if "=" in line:
+                k, v = line.strip().split("=", 1)
+                params[k] = v
+        out["inverter"][name] = {"ps_correlator": vals, "input": params, "tolerance_percent": 0.1,
+                                 "where": f"executables/tests/{name}, {inp}"}
     return out
 
 
