@@ -128,10 +128,13 @@ SIGNATURES = {
                                            C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
     "c2q_perform_inversion_eo_fields": (C.c_int, [_P, _P, _P, _P, _D, C.c_double, C.c_double, C.c_int,
                                                   C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
-    "c2q_correlator_ps": (C.c_int, [C.POINTER(_P), C.POINTER(_P), C.c_int, C.c_double, _D]),
+    "c2q_correlator_ps": (C.c_int, [C.POINTER(_P), C.POINTER(_P), C.c_int, C.c_double, C.c_int, _D]),
     "c2q_gauge_generate": (C.c_int, [_D, C.c_int, C.c_int, C.c_double, C.c_ulonglong]),
     "c2q_source_generate": (C.c_int, [_D, C.c_size_t, C.c_int, C.c_ulonglong]),
     "c2q_spinor_eo_source": (C.c_int, [_P, C.c_int, C.c_ulonglong]),
+    "c2q_ildg_read": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                C.POINTER(C.c_int), C.c_char_p, C.c_int, C.POINTER(C.c_uint), C.POINTER(C.c_uint),
+                                C.POINTER(C.c_int)]),
     "c2q_server_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_int]),
     "c2q_server_add_gauge": (C.c_int, [_P, C.c_ulonglong, C.POINTER(CLattice), _D]),
     "c2q_server_submit": (C.c_int, [_P, C.POINTER(CRequest), C.POINTER(C.c_longlong)]),

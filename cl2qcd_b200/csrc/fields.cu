@@ -1038,39 +1038,44 @@ C2Q_EXPORT int c2q_spinor_eo_source(c2q_spinor_eo* f, int kind, unsigned long lo
     return C2Q_OK;
 }
 
-// Pseudoscalar correlator from point sources in the time direction
-// (ocl_kernel/fermionobservables/correlator_ps_point.cl, correlator_ps_t):
-// C(t) = (2 kappa)^2 / NS^3 * sum over the solutions and the sites of time
-// slice t of |phi|^2.  The eo index runs with t slowest, so slice t of each
-// parity is the contiguous range [t NS^3/2, (t+1) NS^3/2).  One block per time
+// Pseudoscalar correlator from point sources
+// (ocl_kernel/fermionobservables/correlator_ps_point.cl: correlator_ps_t,
+// correlator_ps_z): along t, C(t) = (2 kappa)^2 / NS^3 * sum over the solutions
+// and the sites of time slice t of |phi|^2; along z, C(z) = (2 kappa)^2 /
+// (NS^2 NT) * the same sum over the sites with that z.  The eo index runs with
+// t slowest and x fastest, so in each parity the sites of time slice t are the
+// range [t NS^3/2, (t+1) NS^3/2) and those of a z slice are, for every t, the
+// range of NS^2/2 indices starting at (NS^2 z + NS^3 t)/2.  One block per
 // slice sums in a fixed order: deterministic.
 constexpr int CORR_THREADS = 256;
-__global__ void correlator_ps_t_kernel(const double2* const* fields, int nfields, int per_slice, int stride,
-                                       double factor, double* out)
+__global__ void correlator_ps_kernel(const double2* const* fields, int nfields, int dir, Geom g, double factor,
+                                     double* out)
 {
-    const int t = blockIdx.x;
-    double acc[1] = {0.0};
+    const int s      = blockIdx.x;  // slice coordinate
+    const int plane  = g.ns * g.ns / 2;
+    const int nsites = dir == 0 ? g.vs_h : plane * g.nt;
+    double acc[1]    = {0.0};
     for (int f = 0; f < nfields; ++f) {
         const double2* p = fields[f];
-        for (int i = threadIdx.x; i < per_slice; i += blockDim.x) {
-            const int site = t * per_slice + i;
+        for (int i = threadIdx.x; i < nsites; i += blockDim.x) {
+            const int site = dir == 0 ? s * g.vs_h + i : (i / plane) * g.vs_h + s * plane + (i % plane);
 #pragma unroll
             for (int k = 0; k < 12; ++k) {
-                const double2 v = p[(size_t)k * stride + site];
+                const double2 v = p[(size_t)k * g.stride + site];
                 acc[0] += v.x * v.x + v.y * v.y;
             }
         }
     }
     __shared__ double smem[32];
     block_sum<1>(acc, smem);
-    if (threadIdx.x == 0) out[t] = factor * acc[0];
+    if (threadIdx.x == 0) out[s] = factor * acc[0];
 }
 
 C2Q_EXPORT int c2q_correlator_ps(const c2q_spinor_eo* const* even, const c2q_spinor_eo* const* odd, int n,
-                                 double kappa, double* out)
+                                 double kappa, int direction, double* out)
 {
-    if (!even || !odd || n < 1 || !out || !even[0]) return C2Q_BAD_ARG;
-    c2q_ctx* ctx = even[0]->ctx;
+    if (!even || !odd || n < 1 || !out || !even[0] || (direction != 0 && direction != 3)) return C2Q_BAD_ARG;
+    c2q_ctx* ctx  = even[0]->ctx;
     const Geom& g = even[0]->geom;
     std::vector<const double2*> ptrs;
     for (int k = 0; k < n; ++k) {
@@ -1080,20 +1085,22 @@ C2Q_EXPORT int c2q_correlator_ps(const c2q_spinor_eo* const* even, const c2q_spi
             ptrs.push_back(static_cast<const double2*>(f->data));
         }
     }
+    const int nslices   = direction == 0 ? g.nt : g.ns;
     const size_t pbytes = ptrs.size() * sizeof(void*);
-    const size_t obytes = (size_t)g.nt * sizeof(double);
-    int rc              = ensure_staging(ctx, pbytes + obytes);
+    const size_t obytes = (size_t)nslices * sizeof(double);
+    int rc              = ensure_staging(ctx, ((pbytes + 15) / 16) * 16 + obytes);
     if (rc) return rc;
     char* stage = static_cast<char*>(ctx->staging);
     C2Q_CUDA(ctx, cudaMemcpyAsync(stage, ptrs.data(), pbytes, cudaMemcpyHostToDevice, ctx->stream));
-    // the pointer array is read by the kernel before the host vector goes away
-    const double factor = 2.0 * kappa * 2.0 * kappa / ((double)g.ns * g.ns * g.ns);
+    const double k2     = 2.0 * kappa * 2.0 * kappa;
+    const double factor = direction == 0 ? k2 / ((double)g.ns * g.ns * g.ns) : k2 / ((double)g.ns * g.ns * g.nt);
     double* dout        = reinterpret_cast<double*>(stage + ((pbytes + 15) / 16) * 16);
-    correlator_ps_t_kernel<<<g.nt, CORR_THREADS, 0, ctx->stream>>>(
-        reinterpret_cast<const double2* const*>(stage), (int)ptrs.size(), g.vs_h, g.stride, factor, dout);
+    correlator_ps_kernel<<<nslices, CORR_THREADS, 0, ctx->stream>>>(reinterpret_cast<const double2* const*>(stage),
+                                                                    (int)ptrs.size(), direction, g, factor, dout);
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     C2Q_CUDA(ctx, cudaMemcpyAsync(out, dout, obytes, cudaMemcpyDeviceToHost, ctx->stream));
+    // the pointer array (host vector) must stay alive until the copy has been consumed
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return C2Q_OK;
 }

@@ -491,11 +491,12 @@ def point_source_full(lattice: Lattice, k: int, x: int = 0, y: int = 0, z: int =
 
 def inverter_ps_correlator(system: System, gf: Gaugefield, params: SolverParameters, add: AdditionalParameters,
                            n_sources: int = 12, position=(0, 0, 0, 0), action: str = "twistedmass",
-                           reports: list | None = None) -> np.ndarray:
+                           reports: list | None = None, direction: int = 3) -> np.ndarray:
     """The inverter's point-source measurement (physics/observables/wilsonTwoFlavourCorrelators.cpp:
     measureTwoFlavourDoubletCorrelatorsOnGaugefieldAndWriteToFile with the default 12 point
     sources): perform_inversion (eo) of each spin-colour point source, results kept on the
-    device, and the pseudoscalar correlator C(t) contracted on the GPU."""
+    device, and the pseudoscalar correlator contracted on the GPU along z (direction 3,
+    the reference's default correlatorDirection) or t (direction 0)."""
     lib = system.lib
     L_ = gf.lattice
     act = L.WILSON if action.lower() == "wilson" else L.TWISTEDMASS
@@ -514,11 +515,49 @@ def inverter_ps_correlator(system: System, gf: Gaugefield, params: SolverParamet
         if rc == L.DID_NOT_SOLVE:
             raise SolverDidNotSolve(rep.iterations)
         _check(rc, system.h, lib)
-    out = np.zeros(L_.nt)
+    out = np.zeros(L_.nt if direction == 0 else L_.ns)
     ae = (C.c_void_p * n_sources)(*[f.h for f in evens])
     ao = (C.c_void_p * n_sources)(*[f.h for f in odds])
-    _check(lib.c2q_correlator_ps(ae, ao, n_sources, add.kappa, out), system.h, lib)
+    _check(lib.c2q_correlator_ps(ae, ao, n_sources, add.kappa, direction, out), system.h, lib)
     return out
+
+
+def read_ildg(path: str):
+    """A gauge configuration in ILDG/LIME format (the reference's ildg_io reader):
+    returns (ns, nt, Matrixsu3[4V] as float64 (4V, 18), info) with info holding the
+    precision, the xlf-info text and the SciDAC checksum (computed, and whether it
+    matches the recorded one: 1 yes, 0 no, -1 not recorded)."""
+    lib = L.load()
+    ns, nt, prec, st = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    a, b = C.c_uint(), C.c_uint()
+    p = path.encode()
+    _check(lib.c2q_ildg_read(p, None, 0, C.byref(ns), C.byref(nt), C.byref(prec), None, 0, None, None, None))
+    aos = np.zeros((4 * ns.value ** 3 * nt.value, 18))
+    text = C.create_string_buffer(4096)
+    _check(lib.c2q_ildg_read(p, aos.ctypes.data, aos.size, C.byref(ns), C.byref(nt), C.byref(prec), text, 4096,
+                             C.byref(a), C.byref(b), C.byref(st)))
+    info = {"precision": prec.value, "xlf_info": text.value.decode(errors="replace"), "suma": a.value,
+            "sumb": b.value, "checksum_status": st.value}
+    return ns.value, nt.value, aos, info
+
+
+def plaquette(lattice: Lattice, aos: np.ndarray) -> float:
+    """Average plaquette (1/3) Re tr U_mu(x) U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+ over the
+    6 planes and all sites, from a host Matrixsu3[4V] (mu 0 = time)."""
+    ns, nt = lattice.ns, lattice.nt
+    U = aos.reshape(nt, ns, ns, ns, 4, 3, 3, 2)  # [t][z][y][x][mu][row][col][re,im]
+    U = U[..., 0] + 1j * U[..., 1]
+    axis = {0: 0, 1: 3, 2: 2, 3: 1}  # direction -> array axis (t, z, y, x)
+    tot = 0.0
+    for mu in range(4):
+        for nu in range(mu + 1, 4):
+            a = U[..., mu, :, :]
+            b = np.roll(U[..., nu, :, :], -1, axis=axis[mu])
+            c = np.roll(U[..., mu, :, :], -1, axis=axis[nu])
+            d = U[..., nu, :, :]
+            p_ = a @ b @ np.conj(np.swapaxes(c, -1, -2)) @ np.conj(np.swapaxes(d, -1, -2))
+            tot += np.trace(p_, axis1=-2, axis2=-1).real.sum()
+    return tot / (6 * 3 * lattice.vol)
 
 
 # ---------------- inputs ----------------

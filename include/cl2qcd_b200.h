@@ -293,13 +293,16 @@ C2Q_EXPORT int c2q_perform_inversion_eo(c2q_ctx* ctx, double* result, const c2q_
 C2Q_EXPORT int c2q_perform_inversion_eo_fields(c2q_ctx* ctx, c2q_spinor_eo* out_even, c2q_spinor_eo* out_odd,
                                                const c2q_gauge* g, const double* source, double kappa, double mubar,
                                                int action, const c2q_solver_params* p, c2q_solve_report* report);
-/* Pseudoscalar correlator from point sources in the time direction
+/* Pseudoscalar correlator from point sources
  * (physics/observables/wilsonTwoFlavourCorrelators.cpp:162-415 with
- * ocl_kernel/fermionobservables/correlator_ps_point.cl correlator_ps_t):
- * out[t] = (2 kappa)^2 / NS^3 * sum_k sum_{x in slice t} |phi_k(x)|^2 over the n
- * full solutions phi_k = (even[k], odd[k]); out is a host array of NT doubles. */
+ * ocl_kernel/fermionobservables/correlator_ps_point.cl correlator_ps_t / _z):
+ * direction 0: out[t] = (2 kappa)^2 / NS^3 * sum_k sum_{x in slice t} |phi_k(x)|^2;
+ * direction 3 (the reference's default correlatorDirection, meta/parametersObs.cpp:72):
+ * out[z] = (2 kappa)^2 / (NS^2 NT) * sum_k sum_{x with that z} |phi_k(x)|^2,
+ * over the n full solutions phi_k = (even[k], odd[k]); out is a host array of
+ * NT (direction 0) or NS (direction 3) doubles. */
 C2Q_EXPORT int c2q_correlator_ps(const c2q_spinor_eo* const* even, const c2q_spinor_eo* const* odd, int n,
-                                 double kappa, double* out);
+                                 double kappa, int direction, double* out);
 
 /* ---------------- inputs ---------------- */
 /* Seeded synthetic gauge field U = exp(i eps H), H traceless Hermitian with
@@ -309,6 +312,14 @@ C2Q_EXPORT int c2q_gauge_generate(double* aos, int ns, int nt, double eps, unsig
 /* Seeded sources into host arrays of n_sites spinors:
  * kind 0 = Z2 noise ((+-1 +-i)/sqrt 2 per component), 1 = Gaussian (complex N(0,1) per component). */
 C2Q_EXPORT int c2q_source_generate(double* aos, size_t n_sites, int kind, unsigned long long seed);
+/* Gauge configuration in ILDG format in a LIME file (what the reference reads
+ * with ildg_io/ildgIo_gaugefield.cpp:44-76, copy_gaugefield_from_ildg_format
+ * :158-221): aos receives Matrixsu3[4V] (link mu + 4*site, mu 0 = time); with
+ * aos = NULL only ns / nt / precision are read.  info (may be NULL) receives the
+ * xlf-info text; checksum_status: 1 the recorded SciDAC checksum matches the
+ * data, 0 it does not, -1 none recorded; suma / sumb: the checksum of the data. */
+C2Q_EXPORT int c2q_ildg_read(const char* path, double* aos, size_t aos_len, int* ns, int* nt, int* precision,
+                             char* info, int info_len, unsigned* suma, unsigned* sumb, int* checksum_status);
 /* The same sources generated in place on the device into an FP64 eo field
  * (Z2 bit-identical to c2q_source_generate; Gaussian equal to rounding). */
 C2Q_EXPORT int c2q_spinor_eo_source(c2q_spinor_eo* f, int kind, unsigned long long seed);

@@ -11,7 +11,11 @@ reference tree and the oracle built; the fixtures themselves are committed).
    * hardware/code/fermions_test.cpp: the closed form of the dslash_eo
      kernel test in theta and the chemical potential, and the
      M_tm_sitediagonal family per-site constants.
-2. ref_outputs.npz -- outputs of the reference's own kernels (oracle/_ref/
+2. conf00200.npz -- the reference's ILDG test configuration ildg_io/conf.00200
+   decoded by this project's ILDG reader (Matrixsu3[4V], float64), for the
+   known answers that are defined on it (the second blocks of explicit_test.cpp
+   and fermionmatrix_test.cpp, inverter_test_ref2);
+3. ref_outputs.npz -- outputs of the reference's own kernels (oracle/_ref/
    libc2q_ref.so, compiled from the reference sources) on small seeded
    inputs, used to pin the restated oracle and the CUDA path.
 
@@ -80,6 +84,22 @@ def extract_kats(ref: str) -> dict:
     out["tm_sitediagonal_per_site"] = {"values": diag, "kappa": 0.123456, "mu": 0.123456,
                                        "fill": "ascendingComplex", "lattice": [4, 8],
                                        "where": "hardware/code/fermions_test.cpp:69-104,483-507"}
+    # second blocks of explicit_test.cpp: the full-lattice operators on the ILDG
+    # configuration ildg_io/conf.00200 (nTime 4, default kappa 0.125, mu 0.006)
+    out["explicit_conf00200"] = {}
+    for m in re.finditer(r"BOOST_AUTO_TEST_CASE\((\w+)\)(.*?)(?=BOOST_AUTO_TEST_CASE|\Z)", ex, re.S):
+        name, body = m.group(1), m.group(2)
+        if "conf.00200" not in body:
+            continue
+        second = body.split("conf.00200", 1)[1]
+        seeds = re.findall(r"pseudo_randomize<Spinorfield, spinor>\(&(sf\d), (\d+)\)", second)
+        refs = re.findall(r"BOOST_CHECK_CLOSE\(squarenorm\(\w+\), ([-+0-9.eE]+), 0\.01\)", second)
+        fn = re.findall(r"physics::fermionmatrix::(\w+)\(&sf2, gf, sf1", second)
+        if seeds and refs and fn:
+            out["explicit_conf00200"][name] = {"seeds": {k: int(v) for k, v in seeds},
+                                               "refs": [float(r) for r in refs[:2]], "operator": fn[0],
+                                               "kappa": 0.125, "mu": 0.006, "lattice": [4, 4],
+                                               "where": "physics/fermionmatrix/explicit_test.cpp"}
     # integration references of the inverter executable (executables/tests/testInverter.py:
     # the pseudoscalar correlator lines, compared at 0.1 %), with their input files
     out["inverter"] = {}
@@ -113,9 +133,24 @@ def make_ref_outputs(path):
     np.savez_compressed(path, **data)
 
 
+def decode_conf00200(ref: str) -> dict:
+    """conf.00200 (4^4, the reference's ILDG test configuration) through this
+    project's ILDG reader, stored as the reference's host layout Matrixsu3[4V]."""
+    import cl2qcd_b200 as c2q
+    ns, nt, aos, info = c2q.host.read_ildg(os.path.join(ref, "ildg_io/conf.00200"))
+    np.savez_compressed(os.path.join(HERE, "conf00200.npz"), gauge=aos, ns=ns, nt=nt)
+    plaq = re.findall(r"plaquette = ([0-9.]+)", info["xlf_info"])
+    return {"ns": ns, "nt": nt, "precision": info["precision"], "suma": info["suma"], "sumb": info["sumb"],
+            "checksum_status": info["checksum_status"],
+            "plaquette_recorded": float(plaq[0]) if plaq else None,
+            "plaquette": c2q.host.plaquette(c2q.Lattice(ns, nt), aos),
+            "where": "ildg_io/conf.00200 (xlf-info, scidac-checksum records)"}
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     kats = extract_kats(ref)
+    kats["ildg_conf00200"] = decode_conf00200(ref)
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
         json.dump(kats, f, indent=1, sort_keys=True)
     make_ref_outputs(os.path.join(HERE, "ref_outputs.npz"))

@@ -1,11 +1,13 @@
-"""GPU: the inverter's measurement path against the reference's integration test.
+"""GPU: the inverter's measurement path against the reference's integration tests.
 
-executables/tests/inverter_test_ref (input inverter_test_input_1): 4^4 cold
-gauge field, twisted mass kappa 0.15, mu 4, periodic boundaries, the 12 default
-point sources at the origin, eo perform_inversion of each (result kept on the
-device), pseudoscalar correlator in t contracted on the GPU.  The reference's
-test compares at 0.1 %; the solvers it runs (bicgstab, cg, bicgstab_save) are
-all checked here, and the correlator agrees with the oracle to 1e-9.
+executables/tests/inverter_test_ref (inverter_test_input_1: 4^4 cold gauge field)
+and inverter_test_ref2 (inverter_test_input_2: the ILDG configuration
+conf.00200, decoded by this project's reader into tests/golden/conf00200.npz):
+twisted mass kappa 0.15, mu 4, periodic boundaries, the 12 default point sources
+at the origin, eo perform_inversion of each (result kept on the device), the
+pseudoscalar correlator along z (the reference's default direction) contracted on
+the GPU.  The reference's test compares at 0.1 %; the solvers it runs
+(bicgstab, cg, bicgstab_save) are all checked here, at 1e-9.
 """
 import json
 import os
@@ -19,14 +21,18 @@ KATS = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "
 
 
 @pytest.mark.parametrize("solver", ["bicgstab", "cg", "bicgstab_save"])
-def test_ps_correlator_matches_inverter_reference(system, solver):
+@pytest.mark.parametrize("name", ["inverter_test_ref", "inverter_test_ref2"])
+def test_ps_correlator_matches_inverter_reference(system, solver, name):
     import cl2qcd_b200 as c2q
-    ref = KATS["inverter"]["inverter_test_ref"]
+    ref = KATS["inverter"][name]
     ns, nt = int(ref["input"]["nSpace"]), int(ref["input"]["nTime"])
     kappa, mu = float(ref["input"]["kappa"]), float(ref["input"]["mu"])
     L = c2q.Lattice(ns, nt, 0.0, 0.0)
-    g = np.zeros((4 * L.vol, 18))
-    g[:, 0] = g[:, 8] = g[:, 16] = 1.0  # startCondition=cold
+    if ref["input"]["startCondition"] == "cold":
+        g = np.zeros((4 * L.vol, 18))
+        g[:, 0] = g[:, 8] = g[:, 16] = 1.0
+    else:  # initialConf=conf.00200
+        g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "conf00200.npz"))["gauge"]
     gf = c2q.Gaugefield(system, L, g)
     params = c2q.SolverParameters(solver=solver, prec=1e-23, cgmax=1000)
     reps = []
@@ -38,7 +44,7 @@ def test_ps_correlator_matches_inverter_reference(system, solver):
 
 
 def test_correlator_kernel_matches_numpy(system):
-    """The contraction on random fields: C(t) = (2 kappa)^2 / NS^3 sum |phi|^2 per slice."""
+    """The contraction on random fields, along t and along z."""
     import cl2qcd_b200 as c2q
     L = c2q.Lattice(6, 8, 0.0, 0.0)
     rng = np.random.default_rng(5)
@@ -50,10 +56,14 @@ def test_correlator_kernel_matches_numpy(system):
         ev.append(e)
         od.append(o)
     import ctypes as C
-    out = np.zeros(L.nt)
     lib = system.lib
-    rc = lib.c2q_correlator_ps((C.c_void_p * 3)(*[e.h for e in ev]), (C.c_void_p * 3)(*[o.h for o in od]), 3, 0.13,
-                               out)
-    assert rc == 0
-    expect = sum((f ** 2).sum(axis=1).reshape(L.nt, L.ns ** 3).sum(axis=1) for f in fulls) * (0.26 ** 2) / L.ns ** 3
+    ae, ao = (C.c_void_p * 3)(*[e.h for e in ev]), (C.c_void_p * 3)(*[o.h for o in od])
+    out = np.zeros(L.nt)
+    assert lib.c2q_correlator_ps(ae, ao, 3, 0.13, 0, out) == 0
+    n2 = [(f ** 2).sum(axis=1).reshape(L.nt, L.ns, L.ns, L.ns) for f in fulls]  # [t][z][y][x]
+    expect = sum(a.sum(axis=(1, 2, 3)) for a in n2) * (0.26 ** 2) / L.ns ** 3
+    np.testing.assert_allclose(out, expect, rtol=1e-13)
+    out = np.zeros(L.ns)
+    assert lib.c2q_correlator_ps(ae, ao, 3, 0.13, 3, out) == 0
+    expect = sum(a.sum(axis=(0, 2, 3)) for a in n2) * (0.26 ** 2) / (L.ns ** 2 * L.nt)
     np.testing.assert_allclose(out, expect, rtol=1e-13)

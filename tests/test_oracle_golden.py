@@ -195,8 +195,8 @@ def test_oracle_inversion_solves_full_system(port, O):
 def test_oracle_reproduces_inverter_integration_reference(request, O, kind):
     """executables/tests/inverter_test_ref with inverter_test_input_1: 4^4 cold gauge field,
     twisted mass kappa 0.15, mu 4, periodic boundaries, the 12 default point sources at
-    the origin, eo perform_inversion, pseudoscalar correlator in t (testInverter.py
-    compares at 0.1 %)."""
+    the origin, eo perform_inversion, pseudoscalar correlator in the default direction
+    z (testInverter.py compares at 0.1 %)."""
     ref = KATS["inverter"]["inverter_test_ref"]
     o = _oracle(request, kind)
     ns, nt = int(ref["input"]["nSpace"]), int(ref["input"]["nTime"])
@@ -210,7 +210,8 @@ def test_oracle_reproduces_inverter_integration_reference(request, O, kind):
         src[0, 2 * (3 * (k % 4) + k // 4)] = 1.0
         phi, _, _ = o.perform_inversion_eo(src, g, kappa, 2 * kappa * mu, O.TWISTEDMASS,
                                            O.SolverParams(prec=1e-23, cgmax=1000, solver=2))
-        C += (phi ** 2).sum(axis=1).reshape(nt, ns ** 3).sum(axis=1)
-    C *= (2 * kappa) ** 2 / ns ** 3
+        # the inverter's default correlator direction is z (meta/parametersObs.cpp:72, correlator_ps_z)
+        C += (phi ** 2).sum(axis=1).reshape(nt, ns, ns, ns).sum(axis=(0, 2, 3))
+    C *= (2 * kappa) ** 2 / (ns * ns * nt)
     np.testing.assert_allclose(C, ref["ps_correlator"], rtol=ref["tolerance_percent"] / 100)
     np.testing.assert_allclose(C, ref["ps_correlator"], rtol=1e-9)  # far inside the reference's tolerance
