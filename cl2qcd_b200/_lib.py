@@ -22,6 +22,7 @@ OP_AEE, OP_AEE_MINUS, OP_QPLUS_EO, OP_QMINUS_EO, OP_QPLUSQMINUS_EO, OP_AEE_AND_G
 DIAG_M_TM, DIAG_M_TM_INVERSE, DIAG_M_TM_MINUS, DIAG_M_TM_INVERSE_MINUS, DIAG_M_TM_AND_GAMMA5, \
     DIAG_M_TM_MINUS_AND_GAMMA5 = range(6)
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_BICGSTAB_SAVE = 1, 2, 3
+FULL_M_TM_PLUS, FULL_M_TM_MINUS, FULL_QPLUS, FULL_QMINUS, FULL_QPLUSQMINUS = range(5)
 
 
 class CLattice(C.Structure):
@@ -108,6 +109,7 @@ SIGNATURES = {
     "c2q_tm_sitediagonal": (C.c_int, [_P, _P, C.c_double, C.c_int]),
     "c2q_gamma5_eo": (C.c_int, [_P]),
     "c2q_apply_eo": (C.c_int, [C.c_int, _P, _P, _P, C.c_double, C.c_double, C.c_int, C.c_int]),
+    "c2q_apply_full": (C.c_int, [C.c_int, _P, _P, _P, _P, _P, C.c_double, C.c_double, C.c_int]),
     "c2q_saxpy": (C.c_int, [_P, C.c_double, C.c_double, _P, _P]),
     "c2q_saxpy_AND_gamma5_eo": (C.c_int, [_P, C.c_double, C.c_double, _P, _P]),
     "c2q_sax": (C.c_int, [_P, C.c_double, C.c_double, _P]),

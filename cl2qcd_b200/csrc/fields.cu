@@ -1231,6 +1231,55 @@ C2Q_EXPORT int c2q_apply_eo(int op, c2q_spinor_eo* out, const c2q_gauge* g, cons
     return rc;
 }
 
+// Full-lattice (non-eo) operators on a field held as its two parities
+// (physics/fermionmatrix/fermionmatrix.cpp:41-222, explicit.cpp:36-87;
+// ocl_kernel/fermionmatrix_m_tm_plus.cl): M_tm_plus / minus = (1 +/- i mubar g5)
+// - kappa D (for the Wilson action 1 - kappa D), Qplus / Qminus = g5 M_tm_plus /
+// minus, QplusQminus = Qplus Qminus.  Each parity of the output is one fused
+// sweep: the EPI_AXPY epilogue forms f x - h, so the sweep runs with -kappa to
+// give f x - kappa D x.
+static int full_sweeps(c2q_spinor_eo* oe, c2q_spinor_eo* oo, const c2q_gauge* g, const c2q_spinor_eo* ie,
+                       const c2q_spinor_eo* io, double kappa, double mubar, int action, int minus, int g5)
+{
+    c2q_ctx* ctx  = oe->ctx;
+    const int gk  = gkind_for(oe->prec, ctx->rec12);
+    EpiArgs e     = action == C2Q_ACTION_TWISTEDMASS ? diag_epi(mubar, minus ? C2Q_DIAG_M_TM_MINUS : C2Q_DIAG_M_TM, g5)
+                                                      : EpiArgs{1, 0, 1, 0, g5};
+    int rc = launch_dslash(ctx, g, gk, oe, io, /*even sites*/ 0, -kappa, EPI_AXPY, e, ie, DotSpec{});
+    if (!rc) rc = launch_dslash(ctx, g, gk, oo, ie, /*odd sites*/ 1, -kappa, EPI_AXPY, e, io, DotSpec{});
+    return rc;
+}
+
+C2Q_EXPORT int c2q_apply_full(int op, c2q_spinor_eo* out_even, c2q_spinor_eo* out_odd, const c2q_gauge* g,
+                              const c2q_spinor_eo* in_even, const c2q_spinor_eo* in_odd, double kappa, double mubar,
+                              int action)
+{
+    if (!out_even || !out_odd || !g || !in_even || !in_odd) return C2Q_BAD_ARG;
+    c2q_ctx* ctx = out_even->ctx;
+    if (action != C2Q_ACTION_WILSON && action != C2Q_ACTION_TWISTEDMASS)
+        return fail(ctx, C2Q_BAD_ARG, "unknown fermion action (wilson or twistedmass)");
+    for (const c2q_spinor_eo* o : {(const c2q_spinor_eo*)out_even, (const c2q_spinor_eo*)out_odd})
+        if (o == in_even || o == in_odd) return fail(ctx, C2Q_BAD_ARG, "operator output must not alias its input");
+    switch (op) {
+        case C2Q_FULL_M_TM_PLUS: return full_sweeps(out_even, out_odd, g, in_even, in_odd, kappa, mubar, action, 0, 0);
+        case C2Q_FULL_M_TM_MINUS: return full_sweeps(out_even, out_odd, g, in_even, in_odd, kappa, mubar, action, 1, 0);
+        case C2Q_FULL_QPLUS: return full_sweeps(out_even, out_odd, g, in_even, in_odd, kappa, mubar, action, 0, 1);
+        case C2Q_FULL_QMINUS: return full_sweeps(out_even, out_odd, g, in_even, in_odd, kappa, mubar, action, 1, 1);
+        case C2Q_FULL_QPLUSQMINUS: {
+            c2q_spinor_eo te, to;
+            int rc = field_alloc(ctx, out_even->lat, out_even->prec, &te);
+            if (rc) return rc;
+            rc = field_alloc(ctx, out_even->lat, out_even->prec, &to);
+            if (!rc) rc = full_sweeps(&te, &to, g, in_even, in_odd, kappa, mubar, action, 1, 1);
+            if (!rc) rc = full_sweeps(out_even, out_odd, g, &te, &to, kappa, mubar, action, 0, 1);
+            field_free(&te);
+            field_free(&to);
+            return rc;
+        }
+        default: return fail(ctx, C2Q_BAD_ARG, "unknown full-lattice fermion matrix");
+    }
+}
+
 // ---------------------------------------------------------------- BLAS
 static int blas_simple(int op, c2q_spinor_eo* out, double are, double aim, const c2q_spinor_eo* x,
                        double bre, double bim, const c2q_spinor_eo* y, const c2q_spinor_eo* z)

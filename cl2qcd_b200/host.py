@@ -576,6 +576,71 @@ def generate_source(n_sites: int, kind: str, seed: int) -> np.ndarray:
     return out.reshape(n_sites, 24)
 
 
+# ---------------- full-lattice fields and operators ----------------
+class Spinorfield:
+    """physics::lattices::Spinorfield (a full-lattice field, physics/lattices/spinorfield.hpp),
+    held on the device as its two parities (even = sites with x+y+z+t even)."""
+
+    def __init__(self, system: System, lattice: Lattice, aos: np.ndarray | None = None, precision: int = 64):
+        self.system, self.lattice = system, lattice
+        self.even = Spinorfield_eo(system, lattice, precision=precision)
+        self.odd = Spinorfield_eo(system, lattice, precision=precision)
+        if aos is not None:
+            self.load(aos)
+
+    def load(self, aos):
+        aos = np.ascontiguousarray(aos, dtype=np.float64).reshape(-1)
+        assert aos.size == self.lattice.vol * 24
+        _check(self.system.lib.c2q_convert_to_eoprec(self.even.h, self.odd.h, aos), self.system.h, self.system.lib)
+
+    def dump(self):
+        out = np.zeros(self.lattice.vol * 24)
+        _check(self.system.lib.c2q_convert_from_eoprec(out, self.even.h, self.odd.h), self.system.h, self.system.lib)
+        return out.reshape(self.lattice.vol, 24)
+
+
+class Fermionmatrix:
+    """Full-lattice fermion matrices (physics/fermionmatrix/fermionmatrix.hpp, non-eo)."""
+    OP = None
+
+    def __init__(self, action: str = "twistedmass"):
+        self.action = L.WILSON if action.lower() == "wilson" else L.TWISTEDMASS
+
+    def __call__(self, out: Spinorfield, gf, in_: Spinorfield, params: AdditionalParameters):
+        sysm = out.system
+        _check(sysm.lib.c2q_apply_full(self.OP, out.even.h, out.odd.h, gf.h, in_.even.h, in_.odd.h, params.kappa,
+                                       params.mubar, self.action), sysm.h, sysm.lib)
+
+
+class M_tm_plus(Fermionmatrix):
+    OP = L.FULL_M_TM_PLUS
+
+
+class M_tm_minus(Fermionmatrix):
+    OP = L.FULL_M_TM_MINUS
+
+
+class Qplus(Fermionmatrix):
+    OP = L.FULL_QPLUS
+
+
+class Qminus(Fermionmatrix):
+    OP = L.FULL_QMINUS
+
+
+class QplusQminus(Fermionmatrix):
+    OP = L.FULL_QPLUSQMINUS
+
+
+def M_wilson(out: Spinorfield, gf, in_: Spinorfield, kappa: float):
+    """physics::fermionmatrix::M_wilson (explicit.cpp): (1 - kappa D) in."""
+    Fermionmatrix.__call__(M_tm_plus("wilson"), out, gf, in_, AdditionalParameters(kappa, 0.0))
+
+
+def squarenorm_full(x: Spinorfield) -> float:
+    return squarenorm(x.even) + squarenorm(x.odd)
+
+
 # ---------------- serving (no counterpart in the reference) ----------------
 class Server:
     """Request loop on one GPU (c2q_server_*): `slots` worker threads with their

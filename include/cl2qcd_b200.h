@@ -224,6 +224,18 @@ C2Q_EXPORT int c2q_gamma5_eo(c2q_spinor_eo* inout);
  * `merged` = useKernelMergingFermionMatrix (fermionmatrix.cpp:596). */
 C2Q_EXPORT int c2q_apply_eo(int op, c2q_spinor_eo* out, const c2q_gauge* g, const c2q_spinor_eo* in, double kappa,
                             double mubar, int action, int merged);
+/* Full-lattice (non-eo) fermion matrices (physics/fermionmatrix/fermionmatrix.cpp:41-222,
+ * explicit.cpp:36-87) on a field held as its two parities: M_tm_plus / M_tm_minus
+ * (= M_wilson for the Wilson action), Qplus / Qminus = g5 M_tm_plus / minus,
+ * QplusQminus = Qplus Qminus.  The output must not alias the input. */
+#define C2Q_FULL_M_TM_PLUS 0
+#define C2Q_FULL_M_TM_MINUS 1
+#define C2Q_FULL_QPLUS 2
+#define C2Q_FULL_QMINUS 3
+#define C2Q_FULL_QPLUSQMINUS 4
+C2Q_EXPORT int c2q_apply_full(int op, c2q_spinor_eo* out_even, c2q_spinor_eo* out_odd, const c2q_gauge* g,
+                              const c2q_spinor_eo* in_even, const c2q_spinor_eo* in_odd, double kappa, double mubar,
+                              int action);
 
 /* ---------------- eo BLAS (physics/lattices/spinorfield_eo.hpp:148-305) ---------------- */
 C2Q_EXPORT int c2q_saxpy(c2q_spinor_eo* out, double alpha_re, double alpha_im, const c2q_spinor_eo* x,

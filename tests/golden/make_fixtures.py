@@ -84,6 +84,20 @@ def extract_kats(ref: str) -> dict:
     out["tm_sitediagonal_per_site"] = {"values": diag, "kappa": 0.123456, "mu": 0.123456,
                                        "fill": "ascendingComplex", "lattice": [4, 8],
                                        "where": "hardware/code/fermions_test.cpp:69-104,483-507"}
+    # first blocks of explicit_test.cpp for the full-lattice operators (cold gauge field)
+    out["explicit_full_cold"] = {}
+    for m in re.finditer(r"BOOST_AUTO_TEST_CASE\((\w+)\)(.*?)(?=BOOST_AUTO_TEST_CASE|\Z)", ex, re.S):
+        name, body = m.group(1), m.group(2)
+        first = body.split("conf.00200")[0]
+        seeds = re.findall(r"pseudo_randomize<Spinorfield, spinor>\(&(sf\d), (\d+)\)", first)
+        refs = re.findall(r"BOOST_CHECK_CLOSE\(squarenorm\(\w+\), ([-+0-9.eE]+), 0\.01\)", first)
+        fn = re.findall(r"physics::fermionmatrix::(\w+)\(&sf2, gf, sf1", first)
+        nt = re.findall(r"--nTime=(\d+)", first)
+        if seeds and refs and fn and fn[0] in ("M_wilson", "M_tm_plus", "M_tm_minus"):
+            out["explicit_full_cold"][name] = {"seeds": {k: int(v) for k, v in seeds},
+                                               "refs": [float(r) for r in refs[:2]], "operator": fn[0],
+                                               "kappa": 0.125, "mu": 0.006, "lattice": [4, int(nt[0]) if nt else 4],
+                                               "where": "physics/fermionmatrix/explicit_test.cpp"}
     # second blocks of explicit_test.cpp: the full-lattice operators on the ILDG
     # configuration ildg_io/conf.00200 (nTime 4, default kappa 0.125, mu 0.006)
     out["explicit_conf00200"] = {}

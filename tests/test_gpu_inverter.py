@@ -67,3 +67,29 @@ def test_correlator_kernel_matches_numpy(system):
     assert lib.c2q_correlator_ps(ae, ao, 3, 0.13, 3, out) == 0
     expect = sum(a.sum(axis=(0, 2, 3)) for a in n2) * (0.26 ** 2) / (L.ns ** 2 * L.nt)
     np.testing.assert_allclose(out, expect, rtol=1e-13)
+
+
+FM = {"Aee": "OP_AEE", "Aee_minus": "OP_AEE_MINUS", "Qplus_eo": "OP_QPLUS_EO", "Qminus_eo": "OP_QMINUS_EO",
+      "QplusQminus_eo": "OP_QPLUSQMINUS_EO"}
+
+
+@pytest.mark.parametrize("name", sorted(FM))
+def test_fermionmatrix_eo_kats_on_conf00200(system, port, name):
+    """physics/fermionmatrix/fermionmatrix_test.cpp, second block (conf.00200, nTime 4,
+    Wilson, kappa 0.125) through the GPU's c2q_apply_eo, at the reference's 0.01 %."""
+    import cl2qcd_b200 as c2q
+    from cl2qcd_b200 import _lib as L
+    kat = KATS["fermionmatrix_eo"][name]
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "conf00200.npz"))["gauge"]
+    port.set_lattice(4, 4)
+    Lat = c2q.Lattice(4, 4)
+    gf = c2q.Gaugefield(system, Lat, g)
+    src = port.pseudo_randomize(port.vol, kat["seed"])
+    e, o = port.convert_to_eo(src)
+    sf1, sf2 = c2q.Spinorfield_eo(system, Lat, e), c2q.Spinorfield_eo(system, Lat, o)
+    op = getattr(L, FM[name])
+    lib = system.lib
+    assert lib.c2q_apply_eo(op, sf2.h, gf.h, sf1.h, 0.125, 0.0, L.WILSON, 0) == 0
+    assert c2q.host.squarenorm(sf2) == pytest.approx(kat["refs"][2], rel=1e-4)
+    assert lib.c2q_apply_eo(op, sf1.h, gf.h, sf2.h, 0.125, 0.0, L.WILSON, 0) == 0
+    assert c2q.host.squarenorm(sf1) == pytest.approx(kat["refs"][3], rel=1e-4)
