@@ -74,8 +74,9 @@ static void pk_dispatch(const PkParams<P>& prm, int cfg, int nl, int epi, int do
 // epilogue, reduction, phase pattern, batch size, volume) outside stream
 // capture times every configuration -- one warm-up launch, then two timed
 // launches each, with the reductions redirected to scratch so the caller's
-// solver scalars are untouched -- and keeps the fastest.  The launches are
-// idempotent (the output depends only on the inputs), so tuning does not
+// solver scalars are untouched -- and keeps the fastest.  The timed launches
+// are idempotent (the output depends only on the inputs; the in-place CG
+// residual update is timed as the same sweep without it), so tuning does not
 // change results.  Shapes first met inside a graph capture use
 // configuration 0 and are not recorded.
 // A tuning choice c selects the kernel configuration c & 1 and the grid
@@ -86,6 +87,9 @@ template <int P>
 static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int dot, int* cfg)
 {
     *cfg = 0;
+    // the fused CG update changes its residual in place, so its launches are not
+    // repeatable: it takes the choice timed on the same sweep without the update
+    if (dot == DOT_CGR) dot = DOT_NONE;
     if (!ctx->autotune) return C2Q_OK;
     const unsigned m = prm.c.real_mask;
     const int ph     = m == 0xFFu ? 0 : ((m & 0xFCu) == 0xFCu ? 1 : 2);
@@ -203,8 +207,10 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
         // the input (once through L2), the output and the epilogue operands
         const double sp = P == 32 ? 96.0 : 52.0;
         const double lk = (r12 ? 12.0 : 18.0) * (P == 32 ? 4.0 : 2.0);
-        tm.bytes = (double)ref->geom.seo *
-                   (8.0 * lk + B.n * sp * (2.0 + (B.epi == EPI_AXPY ? 1.0 : 0.0) + (B.dot_mode == DOT_Y ? 1.0 : 0.0)));
+        // (the fused CG update stores no output and reads and writes the FP32 residual)
+        const double per_rhs = sp * (2.0 + (B.epi == EPI_AXPY ? 1.0 : 0.0) + (B.dot_mode == DOT_Y ? 1.0 : 0.0)) +
+                               (B.dot_mode == DOT_CGR ? 192.0 - sp : 0.0);
+        tm.bytes = (double)ref->geom.seo * (8.0 * lk + B.n * per_rhs);
         cudaEventRecord(tm.a, ctx->stream);
     }
     pk_dispatch<P>(prm, cfg, nl, B.epi, B.dot_mode, blocks, ctx->stream);
@@ -223,11 +229,15 @@ int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B
     const c2q_spinor_eo* ref = B.out[0];
     const int P              = ref->prec;
     for (int r = 0; r < B.n; ++r) {
-        for (const c2q_spinor_eo* f : {(const c2q_spinor_eo*)B.out[r], B.in[r], B.x[r], B.y[r]}) {
+        const bool cgr = B.dot_mode == DOT_CGR;
+        for (const c2q_spinor_eo* f : {(const c2q_spinor_eo*)B.out[r], B.in[r], B.x[r], cgr ? nullptr : B.y[r]}) {
             if (!f) continue;
             if (f->prec != P || !same_lattice(f->lat, ref->lat))
                 return fail(ctx, C2Q_BAD_ARG, "fields of a batch differ in precision or lattice");
         }
+        if (cgr && (!B.y[r] || B.y[r]->prec != 32 || !same_lattice(B.y[r]->lat, ref->lat) || !B.sc[r] ||
+                    B.epi != EPI_AXPY))
+            return fail(ctx, C2Q_BAD_ARG, "the fused CG update needs an FP32 residual, solver scalars and EPI_AXPY");
         if (!B.in[r] || B.out[r] == B.in[r]) return fail(ctx, C2Q_BAD_ARG, "dslash output must not alias its input");
         if (B.epi == EPI_AXPY && !B.x[r]) return fail(ctx, C2Q_BAD_ARG, "missing axpy operand");
         if (B.dot_mode == DOT_Y && !B.y[r]) return fail(ctx, C2Q_BAD_ARG, "missing dot partner");
@@ -280,7 +290,8 @@ static int aee_sweeps_batch(c2q_ctx* ctx, int n, c2q_spinor_eo* const* out, cons
 int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out, const c2q_gauge* g, int gkind,
                          const c2q_spinor_eo* const* in, double kappa, double mubar, int action,
                          c2q_spinor_eo* const* tmp1, c2q_spinor_eo* const* tmp2, int dot_mode,
-                         const c2q_spinor_eo* const* y, int fin, SolverScalars* const* sc, int* sweeps)
+                         const c2q_spinor_eo* const* y, int fin, SolverScalars* const* sc, int* sweeps,
+                         c2q_spinor_eo* const* r_update)
 {
     if (action != C2Q_ACTION_WILSON && action != C2Q_ACTION_TWISTEDMASS)
         return fail(ctx, C2Q_BAD_ARG, "unknown fermion action (wilson or twistedmass)");
@@ -309,9 +320,17 @@ int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out,
             // reduced from the intermediate in registers, with no operand read
             rc = aee_sweeps_batch(ctx, n, tmp2, g, gkind, in, kappa, mubar, action, 1, 1, tmp1,
                                   self ? DOT_SELF : DOT_NONE, nullptr, fin, sc);
-            if (!rc)
+            if (!rc && self && r_update) {
+                // alpha is known after the second sweep: the last sweep applies r -= alpha A in
+                // and reduces |r|^2 (FIN_CG_BETA) instead of storing A in
+                const c2q_spinor_eo* rr[PK_MAX_RHS];
+                for (int r = 0; r < n; ++r) rr[r] = r_update[r];
+                rc = aee_sweeps_batch(ctx, n, out, g, gkind, mid, kappa, mubar, action, 0, 1, tmp1, DOT_CGR, rr,
+                                      FIN_CG_BETA, sc);
+            } else if (!rc) {
                 rc = aee_sweeps_batch(ctx, n, out, g, gkind, mid, kappa, mubar, action, 0, 1, tmp1,
                                       self ? DOT_NONE : dot_mode, y, fin, sc);
+            }
             if (sweeps) *sweeps += 2;
             break;
         }

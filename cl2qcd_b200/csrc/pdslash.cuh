@@ -242,6 +242,37 @@ __device__ __forceinline__ void stage_link(uint4* st, const char* links, int ss,
     }
 }
 
+// The fused CG update stages the 12 chunks of the slot's FP32 residual in the
+// two epilogue slots: the q = 9 slot (unused by a DOT_CGR sweep) from chunk 0,
+// and, when it is shorter than 12 chunks, the rest of the q = 8 slot after the
+// EPI_AXPY operand (FP16: chunks 7 ..).
+template <int P, int NL>
+struct ResidualPlace {
+    static constexpr int CH     = PkChunks<P, NL>::CH;
+    static constexpr int IN9    = CH < 12 ? CH : 12;        // chunks in the q = 9 slot
+    static constexpr int AFTER8 = P == 16 ? 7 : 12;        // first free chunk of the q = 8 slot
+    static_assert(IN9 + (CH - AFTER8) >= 12, "residual does not fit the epilogue slots");
+};
+template <int P, int NL, int Q>
+__device__ __forceinline__ void stage_residual(uint4* st, const void* r, int ss, int slot)
+{
+    using RP        = ResidualPlace<P, NL>;
+    const uint4* p  = static_cast<const uint4*>(r) + slot;
+    if constexpr (Q == 9) {
+#pragma unroll
+        for (int c = 0; c < RP::IN9; ++c) cp16(st + c * PK_THREADS, p + (size_t)c * ss);
+    } else {
+#pragma unroll
+        for (int c = RP::IN9; c < 12; ++c) cp16(st + (RP::AFTER8 + c - RP::IN9) * PK_THREADS, p + (size_t)c * ss);
+    }
+}
+template <int P, int NL>
+__device__ __forceinline__ uint4 residual_chunk(const uint4* s8, const uint4* s9, int c)
+{
+    using RP = ResidualPlace<P, NL>;
+    return c < RP::IN9 ? s9[c * PK_THREADS] : s8[(RP::AFTER8 + c - RP::IN9) * PK_THREADS];
+}
+
 __device__ __forceinline__ float4 as_f4(uint4 v)
 {
     return make_float4(__uint_as_float(v.x), __uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w));
@@ -449,8 +480,10 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
                 stage_link<P, NL>(st, (back ? bwd_links : fwd_links) + (size_t)(q >> 1) * grp, ss, back ? nb[q] : j);
             } else if constexpr (q == 8) {
                 if (EPI == EPI_AXPY) stage_spinor<P>(st, rr.x, rr.x_norm, ss, j);
+                if (DOT == DOT_CGR) stage_residual<P, NL, 8>(st, rr.y, ss, j);
             } else {
                 if (DOT == DOT_Y) stage_spinor<P>(st, rr.y, rr.y_norm, ss, j);
+                if (DOT == DOT_CGR) stage_residual<P, NL, 9>(st, rr.y, ss, j);
             }
             cp_commit();
         };
@@ -522,12 +555,28 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
                             fma2(a.im, bc2(ms), fma2(xv[c].im, fr, mul2(xv[c].re, fi)))};
             }
         }
-        if constexpr (P == 16)
-            SlotF16::store(rr.out, rr.out_norm, ss, j, acc);
-        else
-            SlotF32::store(rr.out, ss, j, acc);
+        if (DOT != DOT_CGR) {
+            if constexpr (P == 16)
+                SlotF16::store(rr.out, rr.out_norm, ss, j, acc);
+            else
+                SlotF32::store(rr.out, ss, j, acc);
+        }
 
-        if (DOT == DOT_Y) {  // conj(y) out, FP16 y as integers times the per-site scale
+        if (DOT == DOT_CGR) {  // r -= alpha out (r FP32, passed as y, staged in the ring), |r|^2
+            const float ar = (float)rr.sc->alpha[0], ai = (float)rr.sc->alpha[1];
+            float4* rw     = static_cast<float4*>(const_cast<void*>(rr.y));
+            const uint4* s8 = mine + (size_t)((8 % S::STAGES) * S::CH) * PK_THREADS;
+            const uint4* s9 = mine + (size_t)((9 % S::STAGES) * S::CH) * PK_THREADS;
+#pragma unroll
+            for (int c = 0; c < 12; ++c) {
+                C2 r        = c2_from(as_f4(residual_chunk<P, NL>(s8, s9, c)), false);
+                const C2 v  = acc[c];
+                r.re        = fma2(v.re, bc2(-ar), fma2(v.im, bc2(ai), r.re));
+                r.im        = fma2(v.im, bc2(-ar), fma2(v.re, bc2(-ai), r.im));
+                __stcs(rw + (size_t)c * ss + j, c2_to(r));
+                dre         = fma2(r.re, r.re, fma2(r.im, r.im, dre));
+            }
+        } else if (DOT == DOT_Y) {  // conj(y) out, FP16 y as integers times the per-site scale
             C2 yv[12];
             float2 ys;
             staged_operand<P>(mine + (size_t)((9 % S::STAGES) * S::CH) * PK_THREADS, yv, &ys);

@@ -536,6 +536,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
 
     // ---- iterations
     const int per_apply = op == C2Q_OP_QPLUSQMINUS_EO ? 4 : 2;
+    const bool fused    = op == C2Q_OP_QPLUSQMINUS_EO;  // residual update inside the last sweep
     const bool graphs   = P->use_graph && !ctx->profiling;
     BatchGraph graph;
     auto body = [&](const std::vector<int>& A, bool with_p) -> int {
@@ -558,11 +559,21 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
             T1[i]       = t1[k];
             T2[i]       = t2[k];
         }
-        int e = with_p ? mix_p_batch<PB>(ctx, MB) : 0;  // p = r + beta p
+        int e = with_p ? mix_p_batch<PB>(ctx, MB) : 0;  // x += alpha p (previous), p = r + beta p
+        if (fused) {
+            // Q+Q- p: (p, Q+Q- p) = |Q- p|^2 -> alpha after the second sweep, and the last
+            // sweep updates r -= alpha Q+Q- p with |r|^2 -> beta (v is never stored)
+            c2q_spinor_eo* R[PK_MAX_RHS];
+            for (int i = 0; i < m; ++i) R[i] = rs[A[i]];
+            if (!e)
+                e = apply_operator_batch(ctx, op, m, outs, g, gk, ins, kappa, mubar, action, T1, T2, DOT_Y, ins,
+                                         FIN_CG_ALPHA, scs, nullptr, R);
+            return e;
+        }
         if (!e)  // v = A p with (p, v) -> alpha
             e = apply_operator_batch(ctx, op, m, outs, g, gk, ins, kappa, mubar, action, T1, T2, DOT_Y, ins,
                                      FIN_CG_ALPHA, scs, nullptr);
-        if (!e) e = mix_update_batch<PB>(ctx, MB);  // x += alpha p, r -= alpha v, |r|^2 -> beta
+        if (!e) e = mix_update_batch<PB>(ctx, MB);  // r -= alpha v, |r|^2 -> beta
         return e;
     };
     // Pipelined residual monitoring: every iteration copies |r|^2 and the
