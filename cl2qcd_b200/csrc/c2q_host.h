@@ -178,12 +178,13 @@ int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B
 // |Qminus_eo in|^2, which equals it because Qplus_eo = Qminus_eo^dagger).
 // With r_update (QplusQminus_eo, y = in) the last sweep instead applies the CG
 // residual update r[r] -= alpha A in[r] and reduces |r|^2 into sc[r] (FIN_CG_BETA);
-// out[r] is then not written.
+// out[r] is then not written; with x_update as well, the third sweep applies the
+// CG solution update x_update[r] += alpha in[r] (FP32 x_update).
 int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out, const c2q_gauge* g, int gkind,
                          const c2q_spinor_eo* const* in, double kappa, double mubar, int action,
                          c2q_spinor_eo* const* tmp1, c2q_spinor_eo* const* tmp2, int dot_mode,
                          const c2q_spinor_eo* const* y, int fin, SolverScalars* const* sc, int* sweeps,
-                         c2q_spinor_eo* const* r_update = nullptr);
+                         c2q_spinor_eo* const* r_update = nullptr, c2q_spinor_eo* const* x_update = nullptr);
 // an event for per-launch profiling (from the context's pool)
 cudaEvent_t profile_event(c2q_ctx* ctx);
 

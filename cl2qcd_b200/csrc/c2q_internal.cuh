@@ -118,7 +118,10 @@ enum Epilogue : int {
 // DOT_CGR (paired-site sweeps only): the CG residual update fused into the
 // sweep -- r -= alpha out with r the FP32 field passed as y and alpha from the
 // solver scalars, |r|^2 reduced; out itself is not stored.
-enum DotMode : int { DOT_NONE = 0, DOT_Y = 1, DOT_SELF = 2, DOT_CGR = 3 };
+// DOT_XUPD (paired-site EPI_PLAIN / EPI_DIAG sweeps only): no reduction; the
+// CG solution update x += alpha p rides along, p the field passed as x (same
+// precision as the sweep) and x the FP32 field passed as y, at the output slot.
+enum DotMode : int { DOT_NONE = 0, DOT_Y = 1, DOT_SELF = 2, DOT_CGR = 3, DOT_XUPD = 4 };
 
 struct EpiArgs {
     double f1re, f1im, f2re, f2im;  // spin 0,1 factor and spin 2,3 factor

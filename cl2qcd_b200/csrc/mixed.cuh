@@ -91,7 +91,8 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_update_kernel(const MixArgs A
     finish_reduction<2>(dv, ra, smem, rhs, nrhs);
 }
 
-// x += alpha p (the previous iteration's deferred update), then p = r + beta p
+// x += alpha p (the previous iteration's deferred update; skipped when x is
+// null because a sweep applied it), then p = r + beta p
 template <int PB>
 __global__ void __launch_bounds__(MIX_THREADS) mix_p_kernel(const MixArgs A)
 {
@@ -106,15 +107,15 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_p_kernel(const MixArgs A)
     C2 p[12], r[12];
     float2 ps;
     mix_load<PB>(F.p, F.p_norm, A.ss, j, p, &ps);
-    SlotF32::load(F.x, A.ss, j, r);
-    float2 cr = mul2(bc2(ar), ps), ci = mul2(bc2(ai), ps), nci = mul2(bc2(-ai), ps);
+    if (F.x) {
+        SlotF32::load(F.x, A.ss, j, r);
+        const float2 cr = mul2(bc2(ar), ps), ci = mul2(bc2(ai), ps), nci = mul2(bc2(-ai), ps);
 #pragma unroll
-    for (int c = 0; c < 12; ++c) r[c] = caxpy2(r[c], cr, ci, nci, p[c]);
-    SlotF32::store(F.x, A.ss, j, r);
+        for (int c = 0; c < 12; ++c) r[c] = caxpy2(r[c], cr, ci, nci, p[c]);
+        SlotF32::store(F.x, A.ss, j, r);
+    }
     SlotF32::load(F.r, A.ss, j, r);
-    cr  = mul2(bc2(br), ps);
-    ci  = mul2(bc2(bi), ps);
-    nci = mul2(bc2(-bi), ps);
+    const float2 cr = mul2(bc2(br), ps), ci = mul2(bc2(bi), ps), nci = mul2(bc2(-bi), ps);
 #pragma unroll
     for (int c = 0; c < 12; ++c) p[c] = caxpy2(r[c], cr, ci, nci, p[c]);
     mix_store<PB>(F.p, F.p_norm, A.ss, j, p);

@@ -87,9 +87,10 @@ template <int P>
 static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int dot, int* cfg)
 {
     *cfg = 0;
-    // the fused CG update changes its residual in place, so its launches are not
-    // repeatable: it takes the choice timed on the same sweep without the update
-    if (dot == DOT_CGR) dot = DOT_NONE;
+    // the fused CG updates change their residual or solution in place, so their
+    // launches are not repeatable: they take the choice timed on the same sweep
+    // without the update
+    if (dot == DOT_CGR || dot == DOT_XUPD) dot = DOT_NONE;
     if (!ctx->autotune) return C2Q_OK;
     const unsigned m = prm.c.real_mask;
     const int ph     = m == 0xFFu ? 0 : ((m & 0xFCu) == 0xFCu ? 1 : 2);
@@ -181,7 +182,7 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     prm.e          = B.e;
     prm.out_parity = B.out_parity;
     prm.ntiles = (prm.g.H + PK_THREADS - 1) / PK_THREADS;
-    if (B.dot_mode) {  // one partial per tile and right-hand side
+    if (B.dot_mode != DOT_NONE && B.dot_mode != DOT_XUPD) {  // one partial per tile and right-hand side
         int rc0 = ensure_partials(ctx, (size_t)prm.ntiles * B.n);
         if (rc0) return rc0;
     }
@@ -207,9 +208,11 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
         // the input (once through L2), the output and the epilogue operands
         const double sp = P == 32 ? 96.0 : 52.0;
         const double lk = (r12 ? 12.0 : 18.0) * (P == 32 ? 4.0 : 2.0);
-        // (the fused CG update stores no output and reads and writes the FP32 residual)
+        // (the fused residual update stores no output and reads and writes the FP32
+        // residual; the fused solution update reads p and reads and writes the FP32 x)
         const double per_rhs = sp * (2.0 + (B.epi == EPI_AXPY ? 1.0 : 0.0) + (B.dot_mode == DOT_Y ? 1.0 : 0.0)) +
-                               (B.dot_mode == DOT_CGR ? 192.0 - sp : 0.0);
+                               (B.dot_mode == DOT_CGR ? 192.0 - sp : 0.0) +
+                               (B.dot_mode == DOT_XUPD ? 192.0 + sp : 0.0);
         tm.bytes = (double)ref->geom.seo * (8.0 * lk + B.n * per_rhs);
         cudaEventRecord(tm.a, ctx->stream);
     }
@@ -229,15 +232,19 @@ int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B
     const c2q_spinor_eo* ref = B.out[0];
     const int P              = ref->prec;
     for (int r = 0; r < B.n; ++r) {
-        const bool cgr = B.dot_mode == DOT_CGR;
-        for (const c2q_spinor_eo* f : {(const c2q_spinor_eo*)B.out[r], B.in[r], B.x[r], cgr ? nullptr : B.y[r]}) {
+        const bool cgr = B.dot_mode == DOT_CGR, xup = B.dot_mode == DOT_XUPD;
+        for (const c2q_spinor_eo* f :
+             {(const c2q_spinor_eo*)B.out[r], B.in[r], B.x[r], cgr || xup ? nullptr : B.y[r]}) {
             if (!f) continue;
             if (f->prec != P || !same_lattice(f->lat, ref->lat))
                 return fail(ctx, C2Q_BAD_ARG, "fields of a batch differ in precision or lattice");
         }
-        if (cgr && (!B.y[r] || B.y[r]->prec != 32 || !same_lattice(B.y[r]->lat, ref->lat) || !B.sc[r] ||
-                    B.epi != EPI_AXPY))
-            return fail(ctx, C2Q_BAD_ARG, "the fused CG update needs an FP32 residual, solver scalars and EPI_AXPY");
+        if ((cgr || xup) &&
+            (!B.y[r] || B.y[r]->prec != 32 || !same_lattice(B.y[r]->lat, ref->lat) || !B.sc[r] || B.y[r] == B.out[r]))
+            return fail(ctx, C2Q_BAD_ARG, "a fused CG update needs a separate FP32 field and solver scalars");
+        if (cgr && B.epi != EPI_AXPY) return fail(ctx, C2Q_BAD_ARG, "the fused residual update follows EPI_AXPY");
+        if (xup && (B.epi == EPI_AXPY || !B.x[r] || B.x[r] == B.out[r]))
+            return fail(ctx, C2Q_BAD_ARG, "the fused solution update needs p and EPI_PLAIN or EPI_DIAG");
         if (!B.in[r] || B.out[r] == B.in[r]) return fail(ctx, C2Q_BAD_ARG, "dslash output must not alias its input");
         if (B.epi == EPI_AXPY && !B.x[r]) return fail(ctx, C2Q_BAD_ARG, "missing axpy operand");
         if (B.dot_mode == DOT_Y && !B.y[r]) return fail(ctx, C2Q_BAD_ARG, "missing dot partner");
@@ -253,7 +260,8 @@ int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B
 static int aee_sweeps_batch(c2q_ctx* ctx, int n, c2q_spinor_eo* const* out, const c2q_gauge* g, int gkind,
                             const c2q_spinor_eo* const* in, double kappa, double mubar, int action, int minus, int g5,
                             c2q_spinor_eo* const* tmp, int dot_mode, const c2q_spinor_eo* const* y, int fin,
-                            SolverScalars* const* sc)
+                            SolverScalars* const* sc, const c2q_spinor_eo* const* xu_p = nullptr,
+                            c2q_spinor_eo* const* xu_x = nullptr)
 {
     const bool tm = action == C2Q_ACTION_TWISTEDMASS;
     PkBatch B;
@@ -263,9 +271,15 @@ static int aee_sweeps_batch(c2q_ctx* ctx, int n, c2q_spinor_eo* const* out, cons
     B.epi        = tm ? EPI_DIAG : EPI_PLAIN;
     B.e          = tm ? diag_epi(mubar, minus ? C2Q_DIAG_M_TM_INVERSE_MINUS : C2Q_DIAG_M_TM_INVERSE, 0)
                       : EpiArgs{1, 0, 1, 0, 0};
+    B.dot_mode   = xu_x ? DOT_XUPD : DOT_NONE;  // the CG solution update xu_x += alpha xu_p rides along
     for (int r = 0; r < n; ++r) {
         B.out[r] = tmp[r];
         B.in[r]  = in[r];
+        if (xu_x) {
+            B.x[r]  = xu_p[r];
+            B.y[r]  = xu_x[r];
+            B.sc[r] = sc[r];
+        }
     }
     int rc = launch_pdslash(ctx, g, gkind, B);
     if (rc) return rc;
@@ -291,7 +305,7 @@ int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out,
                          const c2q_spinor_eo* const* in, double kappa, double mubar, int action,
                          c2q_spinor_eo* const* tmp1, c2q_spinor_eo* const* tmp2, int dot_mode,
                          const c2q_spinor_eo* const* y, int fin, SolverScalars* const* sc, int* sweeps,
-                         c2q_spinor_eo* const* r_update)
+                         c2q_spinor_eo* const* r_update, c2q_spinor_eo* const* x_update)
 {
     if (action != C2Q_ACTION_WILSON && action != C2Q_ACTION_TWISTEDMASS)
         return fail(ctx, C2Q_BAD_ARG, "unknown fermion action (wilson or twistedmass)");
@@ -322,11 +336,12 @@ int apply_operator_batch(c2q_ctx* ctx, int op, int n, c2q_spinor_eo* const* out,
                                   self ? DOT_SELF : DOT_NONE, nullptr, fin, sc);
             if (!rc && self && r_update) {
                 // alpha is known after the second sweep: the last sweep applies r -= alpha A in
-                // and reduces |r|^2 (FIN_CG_BETA) instead of storing A in
+                // and reduces |r|^2 (FIN_CG_BETA) instead of storing A in, and with x_update
+                // the third sweep applies x += alpha in
                 const c2q_spinor_eo* rr[PK_MAX_RHS];
                 for (int r = 0; r < n; ++r) rr[r] = r_update[r];
                 rc = aee_sweeps_batch(ctx, n, out, g, gkind, mid, kappa, mubar, action, 0, 1, tmp1, DOT_CGR, rr,
-                                      FIN_CG_BETA, sc);
+                                      FIN_CG_BETA, sc, x_update ? in : nullptr, x_update);
             } else if (!rc) {
                 rc = aee_sweeps_batch(ctx, n, out, g, gkind, mid, kappa, mubar, action, 0, 1, tmp1,
                                       self ? DOT_NONE : dot_mode, y, fin, sc);

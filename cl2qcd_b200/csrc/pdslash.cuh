@@ -242,10 +242,11 @@ __device__ __forceinline__ void stage_link(uint4* st, const char* links, int ss,
     }
 }
 
-// The fused CG update stages the 12 chunks of the slot's FP32 residual in the
-// two epilogue slots: the q = 9 slot (unused by a DOT_CGR sweep) from chunk 0,
-// and, when it is shorter than 12 chunks, the rest of the q = 8 slot after the
-// EPI_AXPY operand (FP16: chunks 7 ..).
+// The fused CG updates stage the 12 chunks of the slot's FP32 residual
+// (DOT_CGR) or solution increment (DOT_XUPD) in the two epilogue slots: the
+// q = 9 slot (unused by these sweeps) from chunk 0, and, when it is shorter
+// than 12 chunks, the rest of the q = 8 slot after the spinor operand there
+// (the EPI_AXPY operand or the search direction; FP16: chunks 7 ..).
 template <int P, int NL>
 struct ResidualPlace {
     static constexpr int CH     = PkChunks<P, NL>::CH;
@@ -419,6 +420,8 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
 {
     using S = PkStage<P, NL, CFG>;
     static_assert(S::STAGES == 2 || S::STAGES == 3, "the prologue below issues one or two stages");
+    static_assert(DOT != DOT_XUPD || EPI != EPI_AXPY, "the solution update shares the EPI_AXPY operand slot");
+    constexpr bool RED = DOT != DOT_NONE && DOT != DOT_XUPD;  // a reduction is fused
     extern __shared__ uint4 ring[];
     uint4* mine     = ring + threadIdx.x;
     const PkGeom& g = prm.g;
@@ -479,11 +482,11 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
                 stage_spinor<P>(st, rr.in, rr.in_norm, ss, nb[q]);
                 stage_link<P, NL>(st, (back ? bwd_links : fwd_links) + (size_t)(q >> 1) * grp, ss, back ? nb[q] : j);
             } else if constexpr (q == 8) {
-                if (EPI == EPI_AXPY) stage_spinor<P>(st, rr.x, rr.x_norm, ss, j);
-                if (DOT == DOT_CGR) stage_residual<P, NL, 8>(st, rr.y, ss, j);
+                if (EPI == EPI_AXPY || DOT == DOT_XUPD) stage_spinor<P>(st, rr.x, rr.x_norm, ss, j);
+                if (DOT == DOT_CGR || DOT == DOT_XUPD) stage_residual<P, NL, 8>(st, rr.y, ss, j);
             } else {
                 if (DOT == DOT_Y) stage_spinor<P>(st, rr.y, rr.y_norm, ss, j);
-                if (DOT == DOT_CGR) stage_residual<P, NL, 9>(st, rr.y, ss, j);
+                if (DOT == DOT_CGR || DOT == DOT_XUPD) stage_residual<P, NL, 9>(st, rr.y, ss, j);
             }
             cp_commit();
         };
@@ -592,16 +595,32 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
         } else if (DOT == DOT_SELF) {
 #pragma unroll
             for (int c = 0; c < 12; ++c) dre = fma2(acc[c].re, acc[c].re, fma2(acc[c].im, acc[c].im, dre));
+        } else if (DOT == DOT_XUPD) {  // x += alpha p (x FP32, passed as y; p passed as x; both staged)
+            const float ar  = (float)rr.sc->alpha[0], ai = (float)rr.sc->alpha[1];
+            float4* xw      = static_cast<float4*>(const_cast<void*>(rr.y));
+            const uint4* s8 = mine + (size_t)((8 % S::STAGES) * S::CH) * PK_THREADS;
+            const uint4* s9 = mine + (size_t)((9 % S::STAGES) * S::CH) * PK_THREADS;
+            C2 pv[12];
+            float2 ps;
+            staged_operand<P>(s8, pv, &ps);
+            const float2 cr = mul2(bc2(ar), ps), ci = mul2(bc2(ai), ps), nci = mul2(bc2(-ai), ps);
+#pragma unroll
+            for (int c = 0; c < 12; ++c) {
+                C2 xv = c2_from(as_f4(residual_chunk<P, NL>(s8, s9, c)), false);
+                xv.re = fma2(pv[c].re, cr, fma2(pv[c].im, nci, xv.re));
+                xv.im = fma2(pv[c].im, cr, fma2(pv[c].re, ci, xv.im));
+                __stcs(xw + (size_t)c * ss + j, c2_to(xv));
+            }
         }
     }
-    if (DOT != DOT_NONE) {  // one partial per tile, in tile order
+    if (RED) {  // one partial per tile, in tile order
         double dv[2] = {(double)dre.x + (double)dre.y,
                         ((double)dim.x - (double)dq.x) + ((double)dim.y - (double)dq.y)};
         block_sum<2>(dv, smem);
         store_partial<2>(dv, prm.red, (size_t)tile * nrhs + rhs);
     }
     }  // tiles
-    if (DOT != DOT_NONE) {
+    if (RED) {
         RedArgs ra = prm.red;
         if (rr.sc) ra.sc = rr.sc;
         if (rr.result) ra.result = rr.result;

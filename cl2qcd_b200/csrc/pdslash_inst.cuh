@@ -27,8 +27,9 @@ static void pk_go(const PkParams<P>& prm, int blocks, cudaStream_t s)
 template <int P, int NL, int PH, int CFG>
 static void pk_dispatch_ph(const PkParams<P>& prm, int epi, int dot, int blocks, cudaStream_t s)
 {
-    // (epilogue, reduction): 3 x 3 combinations, and the CG residual update after EPI_AXPY
-    switch (dot == DOT_CGR ? 9 : epi * 3 + dot) {
+    // (epilogue, reduction): 3 x 3 combinations, the CG residual update after
+    // EPI_AXPY and the CG solution update after EPI_PLAIN / EPI_DIAG
+    switch (dot == DOT_CGR ? 9 : dot == DOT_XUPD ? 10 + epi : epi * 3 + dot) {
         case 0: pk_go<P, NL, EPI_PLAIN, DOT_NONE, PH, CFG>(prm, blocks, s); break;
         case 1: pk_go<P, NL, EPI_PLAIN, DOT_Y, PH, CFG>(prm, blocks, s); break;
         case 2: pk_go<P, NL, EPI_PLAIN, DOT_SELF, PH, CFG>(prm, blocks, s); break;
@@ -39,6 +40,8 @@ static void pk_dispatch_ph(const PkParams<P>& prm, int epi, int dot, int blocks,
         case 7: pk_go<P, NL, EPI_AXPY, DOT_Y, PH, CFG>(prm, blocks, s); break;
         case 8: pk_go<P, NL, EPI_AXPY, DOT_SELF, PH, CFG>(prm, blocks, s); break;
         case 9: pk_go<P, NL, EPI_AXPY, DOT_CGR, PH, CFG>(prm, blocks, s); break;
+        case 10: pk_go<P, NL, EPI_PLAIN, DOT_XUPD, PH, CFG>(prm, blocks, s); break;
+        case 11: pk_go<P, NL, EPI_DIAG, DOT_XUPD, PH, CFG>(prm, blocks, s); break;
     }
 }
 

@@ -536,7 +536,10 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
 
     // ---- iterations
     const int per_apply = op == C2Q_OP_QPLUSQMINUS_EO ? 4 : 2;
-    const bool fused    = op == C2Q_OP_QPLUSQMINUS_EO;  // residual update inside the last sweep
+    // QplusQminus_eo: the solution update x_s += alpha p rides in the third sweep
+    // and the residual update in the last one; otherwise x_s += alpha p is
+    // deferred to the next mix_p or to the reliable-update accumulation
+    const bool fused    = op == C2Q_OP_QPLUSQMINUS_EO;
     const bool graphs   = P->use_graph && !ctx->profiling;
     BatchGraph graph;
     auto body = [&](const std::vector<int>& A, bool with_p) -> int {
@@ -559,17 +562,23 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
             T1[i]       = t1[k];
             T2[i]       = t2[k];
         }
-        int e = with_p ? mix_p_batch<PB>(ctx, MB) : 0;  // x += alpha p (previous), p = r + beta p
         if (fused) {
-            // Q+Q- p: (p, Q+Q- p) = |Q- p|^2 -> alpha after the second sweep, and the last
-            // sweep updates r -= alpha Q+Q- p with |r|^2 -> beta (v is never stored)
-            c2q_spinor_eo* R[PK_MAX_RHS];
-            for (int i = 0; i < m; ++i) R[i] = rs[A[i]];
+            // p = r + beta p; then Q+Q- p: (p, Q+Q- p) = |Q- p|^2 -> alpha after the
+            // second sweep, the third sweep updates x_s += alpha p and the last one
+            // r -= alpha Q+Q- p with |r|^2 -> beta (v is never stored)
+            c2q_spinor_eo *R[PK_MAX_RHS], *X[PK_MAX_RHS];
+            for (int i = 0; i < m; ++i) {
+                R[i]     = rs[A[i]];
+                X[i]     = xs[A[i]];
+                MB.xs[i] = nullptr;
+            }
+            int e = with_p ? mix_p_batch<PB>(ctx, MB) : 0;
             if (!e)
                 e = apply_operator_batch(ctx, op, m, outs, g, gk, ins, kappa, mubar, action, T1, T2, DOT_Y, ins,
-                                         FIN_CG_ALPHA, scs, nullptr, R);
+                                         FIN_CG_ALPHA, scs, nullptr, R, X);
             return e;
         }
+        int e = with_p ? mix_p_batch<PB>(ctx, MB) : 0;  // x += alpha p (previous), p = r + beta p
         if (!e)  // v = A p with (p, v) -> alpha
             e = apply_operator_batch(ctx, op, m, outs, g, gk, ins, kappa, mubar, action, T1, T2, DOT_Y, ins,
                                      FIN_CG_ALPHA, scs, nullptr);
@@ -643,7 +652,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 // reliable update in FP64 after iteration `iter`
                 SolverScalars h;
                 rc = read_one(k, &h);
-                if (!rc) rc = accumulate<PB>(ctx, x[k], xs[k], p[k], dsc + k);
+                if (!rc) rc = accumulate<PB>(ctx, x[k], xs[k], p[k], fused ? nullptr : dsc + k);
                 if (!rc)
                     rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, gk64);
                 if (rc) return rc;
@@ -678,7 +687,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         if (S[k].active) {  // out of iterations: keep what was gained
             S[k].iters  = iter;
             S[k].active = false;
-            rc          = accumulate<PB>(ctx, x[k], xs[k], p[k], dsc + k);
+            rc          = accumulate<PB>(ctx, x[k], xs[k], p[k], fused ? nullptr : dsc + k);
             if (rc) return rc;
         }
     const double secs = clock.seconds();
