@@ -559,11 +559,14 @@ def main():
         t64 = e0.elapsed_time(e1) / 1e3
         out["fp64_single_rhs"] = {"solves_per_s": 12 / t64, "iterations": [r["iterations"] for r in reps64],
                                   "true_resid_rel_max": max(r["true_resid_rel"] for r in reps64)}
-        for prec, rec12 in ((32, True), (16, True), (16, False)):
+        # (the inner sweeps run in the temporal gauge by default; the last variant
+        # keeps the plain gauge, for comparison)
+        for prec, rec12, tg, sizes in ((32, True, True, (1, 4, 8, 12)), (16, True, True, (1, 4, 8, 12)),
+                                       (16, False, True, (1, 4, 8, 12)), (16, True, False, (1, 12))):
             Pm = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=prec,
-                                      use_rec12=rec12, use_graph=True)
+                                      use_rec12=rec12, use_graph=True, temporal_gauge=tg)
             res = {}
-            for n in (1, 4, 8, 12):
+            for n in sizes:
                 for x_ in Xs[:n]:
                     x_.zero()
                 c2q.host.cg_multi(Xs[:n], A, gf, Bs[:n], Pm, add)  # warm-up: tuning, graph capture
@@ -586,7 +589,7 @@ def main():
                                "reliable_updates": [r["reliable_updates"] for r in reps_],
                                "true_resid_rel_max": max(r["true_resid_rel"] for r in reps_),
                                "speedup_vs_fp64_single_rhs": (n / tb) / (12 / t64)}
-            out[f"fp{prec}_inner" + ("" if rec12 else "_18real_links")] = res
+            out[f"fp{prec}_inner" + ("" if rec12 else "_18real_links") + ("" if tg else "_plain_gauge")] = res
         return out
 
     mrhs = mrhs_section()

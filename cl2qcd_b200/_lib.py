@@ -34,7 +34,7 @@ class CSolverParams(C.Structure):
     _fields_ = [("solver", C.c_int), ("prec", C.c_double), ("rel_tol", C.c_double), ("cgmax", C.c_int),
                 ("iter_refresh", C.c_int), ("resid_check_every", C.c_int), ("min_iter", C.c_int),
                 ("precision", C.c_int), ("reliable_delta", C.c_double), ("use_rec12", C.c_int),
-                ("use_graph", C.c_int)]
+                ("use_graph", C.c_int), ("use_temporal_gauge", C.c_int)]
 
 
 class CSolveReport(C.Structure):

@@ -75,8 +75,12 @@ struct c2q_gauge {
     c2q_lattice lat{};
     c2q::Geom geom{};
     // [0] FP64 18-real, [1] FP64 12-real, [2] FP32 18-real, [3] FP32 12-real, [4] FP16 12-real,
-    // [5] FP16 18-real
-    c2q::GaugeStore store[6];
+    // [5] FP16 18-real; [6..9] the FP32 / FP16 kinds of the field in the temporal gauge
+    c2q::GaugeStore store[10];
+    // temporal gauge: the transformation G(x) (FP64, [parity][9 lanes][stride])
+    // and the weight of the T hop leaving the last time slice
+    c2q::GaugeStore tg_transform;
+    double tg_lam_re = 1.0, tg_lam_im = 0.0;
 };
 
 struct c2q_spinor_eo {
@@ -91,7 +95,18 @@ struct c2q_spinor_eo {
 
 namespace c2q {
 
-enum GaugeKind { G64 = 0, G64R12 = 1, G32 = 2, G32R12 = 3, G16R12 = 4, G16 = 5 };
+enum GaugeKind {
+    G64 = 0, G64R12 = 1, G32 = 2, G32R12 = 3, G16R12 = 4, G16 = 5,
+    G32TG = 6, G32R12TG = 7, G16R12TG = 8, G16TG = 9,  // the same in the temporal gauge
+    GAUGE_KINDS = 10
+};
+inline bool gkind_is_tg(int k) { return k >= G32TG && k <= G16TG; }
+inline bool gkind_is_r12(int k) { return k == G64R12 || k == G32R12 || k == G16R12 || k == G32R12TG || k == G16R12TG; }
+// the temporal-gauge kind of a FP32 / FP16 kind
+inline int gkind_tg(int k)
+{
+    return k == G32 ? G32TG : k == G32R12 ? G32R12TG : k == G16R12 ? G16R12TG : k == G16 ? G16TG : -1;
+}
 
 // ---- status plumbing ----
 int fail(c2q_ctx* ctx, int code, const std::string& msg);
@@ -118,6 +133,23 @@ int field_alloc(c2q_ctx* ctx, const c2q_lattice& lat, int prec, c2q_spinor_eo* f
 void field_free(c2q_spinor_eo* f);
 size_t field_bytes(const Geom& g, int prec);
 int gauge_ensure(c2q_gauge* g, int kind);  // builds a lower-precision copy on first use
+
+// ---- temporal gauge (tgauge.cu) ----
+// The inner solves of the mixed-precision CG may run on the field transformed
+// by G(x, t) = c^t prod_{t' < t} U_T(x, t') (c the forward T phase): every T
+// link becomes the identity except the one leaving the last time slice, which
+// becomes lambda W (W in SU(3), lambda = c^NT), all hop phases real.  Possible
+// when the T weights are pure phases and the spatial ones real.
+bool tg_applicable(const c2q_lattice& lat);
+// the transformation G and lambda (first use)
+int tg_ensure(c2q_gauge* g);
+// the transformed links as an FP64 9-lane store (the layout of G64) in out
+int tg_links_fp64(c2q_gauge* g, void* out);
+// out (FP32) = G in (FP64), on the sites of parity 1 (those of the CG vectors)
+int tg_to_inner(c2q_ctx* ctx, const c2q_gauge* g, c2q_spinor_eo* out, const c2q_spinor_eo* in);
+// x (FP64) += G^dagger (xs + alpha p) (alpha from sc; sc null: xs only), xs = 0
+int tg_accumulate(c2q_ctx* ctx, const c2q_gauge* g, c2q_spinor_eo* x, c2q_spinor_eo* xs, const c2q_spinor_eo* p,
+                  const SolverScalars* sc);
 int ensure_staging(c2q_ctx* ctx, size_t bytes);
 int ensure_partials(c2q_ctx* ctx, size_t blocks);
 

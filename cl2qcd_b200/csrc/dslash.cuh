@@ -136,7 +136,10 @@ __device__ __forceinline__ void hop_decoded(Cplx<R> acc[12], const Cplx<R> psi[1
 // Phase patterns known at compile time (the common boundary conditions): PH_REAL
 // all hop phases real, PH_TCPLX only the T phases complex (antiperiodic time,
 // periodic space), PH_ANY decided per launch from HopCoef::real_mask.
-enum PhasePattern : int { PH_REAL = 0, PH_TCPLX = 1, PH_ANY = 2 };
+// PH_TG (paired-site sweeps only): the field is in the temporal gauge (every T
+// link is the identity except the one leaving the last time slice, and the T
+// phase sits in the transformation), all hop coefficients are real.
+enum PhasePattern : int { PH_REAL = 0, PH_TCPLX = 1, PH_ANY = 2, PH_TG = 3 };
 
 // One hop: load the neighbour spinor and the link, weight by the hop phase.
 template <int P, int NL, int MU, bool BACK, int PH>

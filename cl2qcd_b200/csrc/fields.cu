@@ -319,36 +319,61 @@ __global__ void gauge_convert16_kernel(const double2* __restrict__ in, uint4* __
 int gauge_ensure(c2q_gauge* g, int kind)
 {
     c2q_ctx* ctx = g->ctx;
+    if (kind < 0 || kind >= GAUGE_KINDS) return fail(ctx, C2Q_BAD_ARG, "bad gauge kind");
     if (g->store[kind].data) return C2Q_OK;
     if (!g->store[G64].data) return fail(ctx, C2Q_BAD_ARG, "gauge field not uploaded");
     const size_t lanes = (size_t)8 * g->geom.stride;
     size_t bytes       = 0;
     switch (kind) {
         case G64R12: bytes = lanes * 6 * 16; break;
-        case G32: bytes = lanes * 9 * 8; break;
-        case G32R12: bytes = lanes * 6 * 8; break;
-        case G16R12: bytes = lanes * 6 * 4; break;
-        case G16: bytes = lanes * 9 * 4; break;
+        case G32: case G32TG: bytes = lanes * 9 * 8; break;
+        case G32R12: case G32R12TG: bytes = lanes * 6 * 8; break;
+        case G16R12: case G16R12TG: bytes = lanes * 6 * 4; break;
+        case G16: case G16TG: bytes = lanes * 9 * 4; break;
         default: return fail(ctx, C2Q_BAD_ARG, "bad gauge kind");
     }
+    if (kind != G64R12 && (g->lat.nt % 4))
+        return fail(ctx, C2Q_BAD_ARG, "FP32 / FP16 links pair the times t and t + NT/2: NT must be a multiple of 4");
+    const double2* src = static_cast<const double2*>(g->store[G64].data);
+    void* tmp          = nullptr;  // temporal gauge: the transformed FP64 links
+    if (gkind_is_tg(kind)) {
+        C2Q_CUDA(ctx, cudaMalloc(&tmp, lanes * 9 * 16));
+        const int rc = tg_links_fp64(g, tmp);
+        if (rc) {
+            cudaFree(tmp);
+            return rc;
+        }
+        src = static_cast<const double2*>(tmp);
+    }
     void* p = nullptr;
-    C2Q_CUDA(ctx, cudaMalloc(&p, bytes));
+    const cudaError_t ea = cudaMalloc(&p, bytes);
+    if (ea != cudaSuccess) {
+        cudaFree(tmp);
+        return cuda_fail(ctx, ea, "cudaMalloc(gauge copy)");
+    }
     const int threads = 256;
     const unsigned blocks = (unsigned)((lanes + threads - 1) / threads);
-    const double2* src    = static_cast<const double2*>(g->store[G64].data);
-    if (kind != G64R12 && (g->lat.nt % 4)) {
-        cudaFree(p);
-        return fail(ctx, C2Q_BAD_ARG, "FP32 / FP16 links pair the times t and t + NT/2: NT must be a multiple of 4");
-    }
     switch (kind) {
         case G64R12: gauge_convert64_kernel<<<blocks, threads, 0, ctx->stream>>>(src, (double2*)p, g->geom); break;
         case G32: gauge_convert32_kernel<9><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
         case G32R12: gauge_convert32_kernel<6><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
         case G16R12: gauge_convert16_kernel<6><<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
         case G16: gauge_convert16_kernel<9><<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
+        case G32TG: gauge_convert32_kernel<9><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
+        case G32R12TG: gauge_convert32_kernel<6><<<blocks, threads, 0, ctx->stream>>>(src, (float4*)p, g->geom); break;
+        case G16R12TG: gauge_convert16_kernel<6><<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
+        case G16TG: gauge_convert16_kernel<9><<<blocks, threads, 0, ctx->stream>>>(src, (uint4*)p, g->geom); break;
     }
     ctx->launches++;
-    C2Q_CUDA(ctx, cudaGetLastError());
+    const cudaError_t ek = cudaGetLastError();
+    if (tmp) {  // stream-ordered: the conversion finishes before the scratch is released
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(tmp);
+    }
+    if (ek != cudaSuccess) {
+        cudaFree(p);
+        return cuda_fail(ctx, ek, "gauge conversion");
+    }
     g->store[kind].data  = p;
     g->store[kind].bytes = bytes;
     return C2Q_OK;
@@ -801,6 +826,7 @@ C2Q_EXPORT int c2q_gauge_destroy(c2q_gauge* g)
     if (!g) return C2Q_OK;
     cudaStreamSynchronize(g->ctx->stream);
     for (auto& s : g->store) cudaFree(s.data);
+    cudaFree(g->tg_transform.data);
     delete g;
     return C2Q_OK;
 }
@@ -808,8 +834,10 @@ C2Q_EXPORT int c2q_gauge_destroy(c2q_gauge* g)
 C2Q_EXPORT size_t c2q_gauge_device_bytes(const c2q_gauge* g)
 {
     size_t b = 0;
-    if (g)
+    if (g) {
         for (auto& s : g->store) b += s.bytes;
+        b += g->tg_transform.bytes;
+    }
     return b;
 }
 
@@ -827,14 +855,15 @@ C2Q_EXPORT int c2q_gauge_upload(c2q_gauge* g, const double* aos)
         (const double2*)ctx->staging, (double2*)g->store[G64].data, g->geom, vol);
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
-    // lower-precision copies are rebuilt from the new links on next use
-    for (int k = 1; k < 5; ++k) {
-        if (g->store[k].data) {
-            C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-            cudaFree(g->store[k].data);
-            g->store[k] = GaugeStore{};
-        }
+    // lower-precision copies (and the temporal gauge) are rebuilt from the new
+    // links on next use
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int k = 1; k < GAUGE_KINDS; ++k) {
+        cudaFree(g->store[k].data);
+        g->store[k] = GaugeStore{};
     }
+    cudaFree(g->tg_transform.data);
+    g->tg_transform = GaugeStore{};
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return C2Q_OK;
 }

@@ -93,7 +93,7 @@ static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int 
     if (dot == DOT_CGR || dot == DOT_XUPD) dot = DOT_NONE;
     if (!ctx->autotune) return C2Q_OK;
     const unsigned m = prm.c.real_mask;
-    const int ph     = m == 0xFFu ? 0 : ((m & 0xFCu) == 0xFCu ? 1 : 2);
+    const int ph     = prm.tg ? 3 : m == 0xFFu ? 0 : ((m & 0xFCu) == 0xFCu ? 1 : 2);
     std::vector<int> key{P, nl, epi, dot, ph, prm.nrhs, 2 * prm.g.H};
     auto it = ctx->tune.find(key);
     if (it != ctx->tune.end()) {
@@ -177,6 +177,18 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     prm.gauge      = g->store[gkind].data;
     prm.g          = pk_geom(ref->geom);
     prm.c          = hop_coef(ref->lat, B.kappa);
+    if (gkind_is_tg(gkind)) {
+        // temporal gauge: the T phases sit in the transformation, the last slice's
+        // T hop carries lambda
+        prm.tg     = 1;
+        prm.lam_re = g->tg_lam_re;
+        prm.lam_im = g->tg_lam_im;
+        for (int d = 0; d < 2; ++d) {
+            prm.c.re[0][d] = 1.0;
+            prm.c.im[0][d] = 0.0;
+        }
+        prm.c.real_mask = 0xFFu;
+    }
     // FP16: links in units of 1/32767 and neighbour spinors in units of norm/32767
     if (P == 16) prm.c.scale *= 1.0 / (32767.0 * 32767.0);
     prm.e          = B.e;
@@ -191,7 +203,7 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     prm.red.result   = ctx->red_result;
     prm.red.sc       = ctx->scalars;
     prm.red.fin      = B.fin;
-    const bool r12   = gkind == G32R12 || gkind == G16R12;  // else 18-real
+    const bool r12   = gkind_is_r12(gkind);  // else 18-real
     const int nl     = r12 ? 6 : 9;
     int choice       = 0;
     int rc           = pk_choose<P>(ctx, prm, nl, B.epi, B.dot_mode, &choice);
@@ -248,6 +260,14 @@ int launch_pdslash(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch& B
         if (!B.in[r] || B.out[r] == B.in[r]) return fail(ctx, C2Q_BAD_ARG, "dslash output must not alias its input");
         if (B.epi == EPI_AXPY && !B.x[r]) return fail(ctx, C2Q_BAD_ARG, "missing axpy operand");
         if (B.dot_mode == DOT_Y && !B.y[r]) return fail(ctx, C2Q_BAD_ARG, "missing dot partner");
+    }
+    const bool links_ok = P == 32 ? (gkind == G32 || gkind == G32R12 || gkind == G32TG || gkind == G32R12TG)
+                                  : (gkind == G16 || gkind == G16R12 || gkind == G16TG || gkind == G16R12TG);
+    if (!links_ok) return fail(ctx, C2Q_BAD_ARG, "gauge precision mismatch");
+    if (gkind_is_tg(gkind)) {  // the instantiations of the mixed-precision CG sweeps
+        const int c = B.dot_mode == DOT_CGR ? 9 : B.dot_mode == DOT_XUPD ? 10 + B.epi : B.epi * 3 + B.dot_mode;
+        if (!(c == 0 || c == 3 || c == 6 || c == 8 || c == 9 || c == 10 || c == 11))
+            return fail(ctx, C2Q_BAD_ARG, "no temporal-gauge sweep with this epilogue and reduction");
     }
     int rc = gauge_ensure(const_cast<c2q_gauge*>(g), gkind);
     if (rc) return rc;

@@ -62,6 +62,8 @@ struct PkParams {
     EpiArgs e;
     int out_parity;
     int ntiles;  // tiles of PK_THREADS slots per right-hand side
+    int tg;                 // the gauge field is in the temporal gauge (PH_TG)
+    double lam_re, lam_im;  // PH_TG: weight of the T hop leaving the last time slice
     RedArgs red;
 };
 
@@ -349,8 +351,9 @@ __device__ __forceinline__ void staged_operand(const uint4* st, C2 q[12], float2
 // One hop from a stage: the neighbour slot (and, for a backward hop, its
 // link) may hold the two sites swapped -- SWP, set for the time hops across
 // the fold.  A forward hop's link sits at the output slot and is never swapped.
+// w: the hop weight of each lane (the two sites) and its negations.
 template <int P, int NL, int MU, bool BACK, bool SWP, bool KREAL>
-__device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, double phre, double phim)
+__device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, const Kc& w)
 {
     using T          = Proj<MU>;
     constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
@@ -360,28 +363,25 @@ __device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, double phre,
     Kc k;
     C2 h[3];
     if constexpr (P == 16) {
-        uint2 w[12];
+        uint2 wd[12];
         float2 nrm;
-        staged_words<SWP>(st, w, &nrm);
-        k.re  = mul2(bc2((float)phre), nrm);
-        k.nre = mul2(bc2((float)-phre), nrm);
+        staged_words<SWP>(st, wd, &nrm);
+        k.re  = mul2(w.re, nrm);
+        k.nre = mul2(w.nre, nrm);
         if (!KREAL) {
-            k.im  = mul2(bc2((float)phim), nrm);
-            k.nim = mul2(bc2((float)-phim), nrm);
+            k.im  = mul2(w.im, nrm);
+            k.nim = mul2(w.nim, nrm);
         }
 #pragma unroll
-        for (int col = 0; col < 3; ++col) h[col] = proj_words<c0>(w[col], w[3 * T::p0 + col]);
+        for (int col = 0; col < 3; ++col) h[col] = proj_words<c0>(wd[col], wd[3 * T::p0 + col]);
         pk_channel<0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
 #pragma unroll
-        for (int col = 0; col < 3; ++col) h[col] = proj_words<c1>(w[3 + col], w[3 * T::p1 + col]);
+        for (int col = 0; col < 3; ++col) h[col] = proj_words<c1>(wd[3 + col], wd[3 * T::p1 + col]);
         pk_channel<1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
     } else {
         C2 psi[12];
         staged_vals<SWP>(st, psi);
-        k.re  = bc2((float)phre);
-        k.nre = bc2((float)-phre);
-        k.im  = bc2((float)phim);
-        k.nim = bc2((float)-phim);
+        k = w;
 #pragma unroll
         for (int col = 0; col < 3; ++col) h[col] = proj_vals<c0>(psi[col], psi[3 * T::p0 + col]);
         pk_channel<0, T::p0, c0, BACK, KREAL>(acc, h, u, k);
@@ -391,21 +391,90 @@ __device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, double phre,
     }
 }
 
+// A half-spinor channel through an identity link: acc_A += k h, acc_PP += conj(c) k h.
+template <int A, int PP, int CK>
+__device__ __forceinline__ void pk_identity_channel(C2 acc[12], const C2 h[3], const Kc& k)
+{
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        acc_add<0, true>(acc[3 * A + r], h[r].re, h[r].im, k);
+        acc_add<ConjUnit<CK>::value, true>(acc[3 * PP + r], h[r].re, h[r].im, k);
+    }
+}
+// A time hop inside the temporal gauge: the link is the identity (no link
+// staged), the weight real and the same for both lanes.  FP16: the launch
+// scale carries the link scale 1/32767 of a stored link, so the weight here
+// carries 32767.
+template <int P, bool BACK>
+__device__ __forceinline__ void pk_hop_id(C2 acc[12], const uint4* st, float wt)
+{
+    using T          = Proj<0>;
+    constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
+    constexpr int c1 = BACK ? NegUnit<T::c1>::value : T::c1;
+    Kc k;
+    C2 h[3];
+    if constexpr (P == 16) {
+        uint2 wd[12];
+        float2 nrm;
+        staged_words<false>(st, wd, &nrm);
+        k.re  = mul2(bc2(wt * 32767.0f), nrm);
+        k.nre = mul2(bc2(-wt * 32767.0f), nrm);
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_words<c0>(wd[col], wd[3 * T::p0 + col]);
+        pk_identity_channel<0, T::p0, c0>(acc, h, k);
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_words<c1>(wd[3 + col], wd[3 * T::p1 + col]);
+        pk_identity_channel<1, T::p1, c1>(acc, h, k);
+    } else {
+        C2 psi[12];
+        staged_vals<false>(st, psi);
+        k.re  = bc2(wt);
+        k.nre = bc2(-wt);
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_vals<c0>(psi[col], psi[3 * T::p0 + col]);
+        pk_identity_channel<0, T::p0, c0>(acc, h, k);
+#pragma unroll
+        for (int col = 0; col < 3; ++col) h[col] = proj_vals<c1>(psi[3 + col], psi[3 * T::p1 + col]);
+        pk_identity_channel<1, T::p1, c1>(acc, h, k);
+    }
+}
+
+__device__ __forceinline__ Kc uniform_weight(double re, double im)
+{
+    return Kc{bc2((float)re), bc2((float)im), bc2((float)-re), bc2((float)-im)};
+}
+
 // hop q = 2 mu + back, with the phase pattern resolved
 template <int P, int NL, int MU, bool BACK, bool SWP, int PH>
 __device__ __forceinline__ void pk_hop_ph(C2 acc[12], const PkParams<P>& prm, const uint4* st)
 {
-    const int d      = BACK ? 1 : 0;
-    const double pre = prm.c.re[MU][d], pim = prm.c.im[MU][d];
-    if (PH == PH_REAL || (PH == PH_TCPLX && MU != 0)) {
-        pk_hop<P, NL, MU, BACK, SWP, true>(acc, st, pre, pim);
+    const int d  = BACK ? 1 : 0;
+    const Kc w   = uniform_weight(prm.c.re[MU][d], prm.c.im[MU][d]);
+    if (PH == PH_REAL || PH == PH_TG || (PH == PH_TCPLX && MU != 0)) {
+        pk_hop<P, NL, MU, BACK, SWP, true>(acc, st, w);
     } else if (PH == PH_TCPLX) {
-        pk_hop<P, NL, MU, BACK, SWP, false>(acc, st, pre, pim);
+        pk_hop<P, NL, MU, BACK, SWP, false>(acc, st, w);
     } else if ((prm.c.real_mask >> (2 * MU + d)) & 1u) {
-        pk_hop<P, NL, MU, BACK, SWP, true>(acc, st, pre, pim);
+        pk_hop<P, NL, MU, BACK, SWP, true>(acc, st, w);
     } else {
-        pk_hop<P, NL, MU, BACK, SWP, false>(acc, st, pre, pim);
+        pk_hop<P, NL, MU, BACK, SWP, false>(acc, st, w);
     }
+}
+
+// A time hop across the fold inside the temporal gauge: one lane crosses the
+// last time slice through its stored link W with the weight lambda (forward)
+// or conj(lambda) (backward), lambda the product of the T phases around the
+// lattice; the other lane steps between two inner slices, where the stored
+// link is the identity and the weight 1.
+template <int P, int NL, bool BACK>
+__device__ __forceinline__ void pk_hop_tg_fold(C2 acc[12], const PkParams<P>& prm, const uint4* st)
+{
+    const float lr = (float)prm.lam_re, li = (float)prm.lam_im;
+    const Kc w     = BACK ? Kc{make_float2(lr, 1.0f), make_float2(-li, 0.0f), make_float2(-lr, -1.0f),
+                           make_float2(li, 0.0f)}
+                          : Kc{make_float2(1.0f, lr), make_float2(0.0f, li), make_float2(-1.0f, -lr),
+                           make_float2(0.0f, -li)};
+    pk_hop<P, NL, 0, BACK, true, false>(acc, st, w);
 }
 
 // bytes per slot of a (parity, mu) group of links in the slot layout
@@ -480,7 +549,10 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
             if constexpr (q < 8) {
                 constexpr bool back = q & 1;
                 stage_spinor<P>(st, rr.in, rr.in_norm, ss, nb[q]);
-                stage_link<P, NL>(st, (back ? bwd_links : fwd_links) + (size_t)(q >> 1) * grp, ss, back ? nb[q] : j);
+                // temporal gauge: the T links between inner slices are the identity
+                if (PH != PH_TG || q >= 2 || (back ? fold_b : fold_f))
+                    stage_link<P, NL>(st, (back ? bwd_links : fwd_links) + (size_t)(q >> 1) * grp, ss,
+                                      back ? nb[q] : j);
             } else if constexpr (q == 8) {
                 if (EPI == EPI_AXPY || DOT == DOT_XUPD) stage_spinor<P>(st, rr.x, rr.x_norm, ss, j);
                 if (DOT == DOT_CGR || DOT == DOT_XUPD) stage_residual<P, NL, 8>(st, rr.y, ss, j);
@@ -505,7 +577,12 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
             const uint4* st = mine + (size_t)((h % S::STAGES) * S::CH) * PK_THREADS;
             constexpr int mu = h >> 1;
             constexpr bool back = h & 1;
-            if constexpr (mu == 0) {
+            if constexpr (mu == 0 && PH == PH_TG) {
+                if (back ? fold_b : fold_f)
+                    pk_hop_tg_fold<P, NL, back>(acc, prm, st);
+                else
+                    pk_hop_id<P, back>(acc, st, 1.0f);
+            } else if constexpr (mu == 0) {
                 if (back ? fold_b : fold_f)
                     pk_hop_ph<P, NL, 0, back, true, PH>(acc, prm, st);
                 else

@@ -45,12 +45,29 @@ static void pk_dispatch_ph(const PkParams<P>& prm, int epi, int dot, int blocks,
     }
 }
 
+// Temporal gauge: the sweeps of the mixed-precision CG on QplusQminus_eo
+// (twisted mass and Wilson) only.
+template <int P, int NL, int CFG>
+static void pk_dispatch_tg(const PkParams<P>& prm, int epi, int dot, int blocks, cudaStream_t s)
+{
+    switch (dot == DOT_CGR ? 9 : dot == DOT_XUPD ? 10 + epi : epi * 3 + dot) {
+        case 0: pk_go<P, NL, EPI_PLAIN, DOT_NONE, PH_TG, CFG>(prm, blocks, s); break;
+        case 3: pk_go<P, NL, EPI_DIAG, DOT_NONE, PH_TG, CFG>(prm, blocks, s); break;
+        case 6: pk_go<P, NL, EPI_AXPY, DOT_NONE, PH_TG, CFG>(prm, blocks, s); break;
+        case 8: pk_go<P, NL, EPI_AXPY, DOT_SELF, PH_TG, CFG>(prm, blocks, s); break;
+        case 9: pk_go<P, NL, EPI_AXPY, DOT_CGR, PH_TG, CFG>(prm, blocks, s); break;
+        case 10: pk_go<P, NL, EPI_PLAIN, DOT_XUPD, PH_TG, CFG>(prm, blocks, s); break;
+        case 11: pk_go<P, NL, EPI_DIAG, DOT_XUPD, PH_TG, CFG>(prm, blocks, s); break;
+    }
+}
 // Phase pattern from HopCoef::real_mask: all real, only T complex, or general.
 template <int P, int NL, int CFG>
 static void pk_dispatch_nl(const PkParams<P>& prm, int epi, int dot, int blocks, cudaStream_t s)
 {
     const unsigned m = prm.c.real_mask;
-    if (m == 0xFFu)
+    if (prm.tg)
+        pk_dispatch_tg<P, NL, CFG>(prm, epi, dot, blocks, s);
+    else if (m == 0xFFu)
         pk_dispatch_ph<P, NL, PH_REAL, CFG>(prm, epi, dot, blocks, s);
     else if ((m & 0xFCu) == 0xFCu)
         pk_dispatch_ph<P, NL, PH_TCPLX, CFG>(prm, epi, dot, blocks, s);

@@ -250,6 +250,9 @@ C2Q_EXPORT int c2q_server_add_gauge(c2q_server* s, unsigned long long gauge_id, 
     // only ever read the gauge object
     const int inner = gkind_for(s->precision, s->rec12);
     if (!rc) rc = gauge_ensure(g, inner);
+    // the inner sweeps of the mixed-precision CG in the temporal gauge, built here
+    // so that solves running side by side only read the gauge object
+    if (!rc && gkind_tg(inner) >= 0 && tg_applicable(g->lat)) rc = gauge_ensure(g, gkind_tg(inner));
     if (!rc && s->rec12) rc = gauge_ensure(g, G64R12);
     if (!rc) rc = c2q_ctx_synchronize(s->loader);
     if (rc) {

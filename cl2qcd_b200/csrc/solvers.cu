@@ -466,7 +466,10 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         t1[k] = &F.f[5 + 2 * n + 4 * k];
         t2[k] = &F.f[6 + 2 * n + 4 * k];
     }
-    const int gk = gkind_for(PB, P->use_rec12);
+    // inner sweeps in the temporal gauge (QplusQminus_eo with pure-phase T weights):
+    // residuals enter as G r, increments leave as G^dagger x_s
+    const bool use_tg = op == C2Q_OP_QPLUSQMINUS_EO && P->use_temporal_gauge && tg_applicable(lat);
+    const int gk      = use_tg ? gkind_tg(gkind_for(PB, P->use_rec12)) : gkind_for(PB, P->use_rec12);
     // FP64 true residuals on 12-real FP64 links when 12-real links were asked
     // for (row 2 rebuilt in FP64: the operator agrees to rounding)
     const int gk64 = P->use_rec12 ? G64R12 : G64;
@@ -500,6 +503,13 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         return C2Q_OK;
     };
 
+    auto to_inner = [&](c2q_spinor_eo* out, const c2q_spinor_eo* in) -> int {
+        return use_tg ? tg_to_inner(ctx, g, out, in) : launch_convert(ctx, out, in);
+    };
+    auto take_out = [&](int k, const SolverScalars* sc) -> int {
+        return use_tg ? tg_accumulate(ctx, g, x[k], xs[k], p[k], sc) : accumulate<PB>(ctx, x[k], xs[k], p[k], sc);
+    };
+
     // ---- initial residuals
     RhsState S[PK_MAX_RHS];
     for (int k = 0; k < n; ++k) {
@@ -511,11 +521,11 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         rc        = norm2(ctx, x[k], &x2);
         if (rc) return rc;
         if (x2 == 0.0) {  // r = b - A 0 = b
-            rc   = launch_convert(ctx, rs[k], b[k]);
+            rc   = to_inner(rs[k], b[k]);
             s.r2 = s.b2;
         } else {
             rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, gk64);
-            if (!rc) rc = launch_convert(ctx, rs[k], r64);
+            if (!rc) rc = to_inner(rs[k], r64);
         }
         if (rc) return rc;
         s.resid = s.r2;
@@ -642,7 +652,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 s.status = C2Q_SOLVER_STUCK;
                 s.iters  = iter;
                 s.active = false;
-                rc       = accumulate<PB>(ctx, x[k], xs[k], p[k], nullptr);  // keep what was gained
+                rc       = take_out(k, nullptr);  // keep what was gained
                 if (rc) return rc;
                 continue;
             }
@@ -652,7 +662,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 // reliable update in FP64 after iteration `iter`
                 SolverScalars h;
                 rc = read_one(k, &h);
-                if (!rc) rc = accumulate<PB>(ctx, x[k], xs[k], p[k], fused ? nullptr : dsc + k);
+                if (!rc) rc = take_out(k, fused ? nullptr : dsc + k);
                 if (!rc)
                     rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, gk64);
                 if (rc) return rc;
@@ -665,7 +675,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                     s.active       = false;
                     continue;
                 }
-                rc = launch_convert(ctx, rs[k], r64);
+                rc = to_inner(rs[k], r64);
                 if (rc) return rc;
                 s.maxrr = std::sqrt(s.r2);
                 // keep the search direction; rescale beta to the true residual
@@ -687,7 +697,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         if (S[k].active) {  // out of iterations: keep what was gained
             S[k].iters  = iter;
             S[k].active = false;
-            rc          = accumulate<PB>(ctx, x[k], xs[k], p[k], fused ? nullptr : dsc + k);
+            rc          = take_out(k, fused ? nullptr : dsc + k);
             if (rc) return rc;
         }
     const double secs = clock.seconds();
@@ -913,6 +923,7 @@ C2Q_EXPORT void c2q_solver_params_default(c2q_solver_params* p)
     p->reliable_delta    = 0.003;
     p->use_rec12         = 0;
     p->use_graph         = 0;
+    p->use_temporal_gauge = 1;
 }
 
 C2Q_EXPORT int c2q_cg(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,

@@ -390,6 +390,7 @@ class SolverParameters:
     reliable_delta: float = 0.003
     use_rec12: bool = False
     use_graph: bool = False
+    temporal_gauge: bool = True
 
     def c(self) -> L.CSolverParams:
         s = {"cg": L.SOLVER_CG, "bicgstab": L.SOLVER_BICGSTAB, "bicgstab_save": L.SOLVER_BICGSTAB_SAVE}
@@ -397,7 +398,7 @@ class SolverParameters:
             raise InvalidParameters(f"unknown solver {self.solver}")
         return L.CSolverParams(s[self.solver], self.prec, self.rel_tol, self.cgmax, self.iter_refresh,
                                self.resid_check_every, self.min_iter, self.precision, self.reliable_delta,
-                               int(self.use_rec12), int(self.use_graph))
+                               int(self.use_rec12), int(self.use_graph), int(self.temporal_gauge))
 
 
 def _solve(fn, x, A, gf, b, params, add, report):
