@@ -225,7 +225,10 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
         const double per_rhs = sp * (2.0 + (B.epi == EPI_AXPY ? 1.0 : 0.0) + (B.dot_mode == DOT_Y ? 1.0 : 0.0)) +
                                (B.dot_mode == DOT_CGR ? 192.0 - sp : 0.0) +
                                (B.dot_mode == DOT_XUPD ? 192.0 + sp : 0.0);
-        tm.bytes = (double)ref->geom.seo * (8.0 * lk + B.n * per_rhs);
+        // (temporal gauge: the T links of a site are read only on the two fold slices
+        // of the slot layout, 2 of NT/2 each way)
+        const double links = gkind_is_tg(gkind) ? 6.0 + 4.0 / ref->lat.nt : 8.0;
+        tm.bytes           = (double)ref->geom.seo * (links * lk + B.n * per_rhs);
         cudaEventRecord(tm.a, ctx->stream);
     }
     pk_dispatch<P>(prm, cfg, nl, B.epi, B.dot_mode, blocks, ctx->stream);
