@@ -131,6 +131,13 @@ SIGNATURES = {
     "c2q_perform_inversion_eo_fields": (C.c_int, [_P, _P, _P, _P, _D, C.c_double, C.c_double, C.c_int,
                                                   C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
     "c2q_correlator_ps": (C.c_int, [C.POINTER(_P), C.POINTER(_P), C.c_int, C.c_double, C.c_int, _D]),
+    "c2q_gaugemomenta_create": (C.c_int, [_P, C.POINTER(CLattice), C.POINTER(_P)]),
+    "c2q_gaugemomenta_destroy": (C.c_int, [_P]),
+    "c2q_gaugemomenta_zero": (C.c_int, [_P]),
+    "c2q_gaugemomenta_upload": (C.c_int, [_P, _D]),
+    "c2q_gaugemomenta_download": (C.c_int, [_P, _D]),
+    "c2q_gaugemomenta_squarenorm": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "c2q_fermion_force_eo": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_double]),
     "c2q_gauge_generate": (C.c_int, [_D, C.c_int, C.c_int, C.c_double, C.c_ulonglong]),
     "c2q_source_generate": (C.c_int, [_D, C.c_size_t, C.c_int, C.c_ulonglong]),
     "c2q_spinor_eo_source": (C.c_int, [_P, C.c_int, C.c_ulonglong]),

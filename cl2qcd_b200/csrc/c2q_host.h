@@ -120,6 +120,8 @@ int cuda_fail(c2q_ctx* ctx, cudaError_t e, const char* where);
 // ---- geometry / coefficients ----
 bool make_geom(const c2q_lattice& lat, Geom* g);
 bool same_lattice(const c2q_lattice& a, const c2q_lattice& b);
+// A constant as the reference passes it in its build options (16 significant digits).
+double as_build_option(double v);
 // Hop coefficients for one launch: -kappa * boundary phase (and chemical potential on T).
 HopCoef hop_coef(const c2q_lattice& lat, double kappa);
 EpiArgs diag_epi(double mubar, int which, int gamma5);

@@ -47,7 +47,7 @@ bool same_lattice(const c2q_lattice& a, const c2q_lattice& b)
 // The reference passes its phases as text build options with 16 significant
 // digits and PI = 3.14159265358979 (hardware/code/opencl_module.cpp:190-203,
 // common_header_files/globaldefs.hpp); the same values are produced here.
-static double as_build_option(double v)
+double as_build_option(double v)
 {
     char buf[64];
     snprintf(buf, sizeof buf, "%.16g", v);

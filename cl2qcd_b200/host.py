@@ -17,6 +17,9 @@ Names, argument meaning and error behaviour follow CL2QCD:
   return the iteration count, raise ``SolverStuck`` / ``SolverDidNotSolve``
   (physics/algorithms/solvers/exceptions.hpp:35-62).
 * ``perform_inversion`` -- physics::algorithms::perform_inversion, eo branch (inversion.cpp:44-242).
+* ``Gaugemomenta``, ``fermion_force``, ``calc_fermion_force``, ``calc_s_fermion`` -- the
+  HMC callers of the eo solvers (physics/lattices/gaugemomenta.hpp,
+  physics/algorithms/fermion_force.cpp, physics/algorithms/metropolis.cpp).
 
 Everything runs in the CUDA library; nothing here computes on the CPU.
 """
@@ -278,8 +281,12 @@ def scalar_product(x, y) -> complex:
 
 
 def squarenorm(x) -> float:
+    """squarenorm of an eo spinor field, or of gauge momenta (the reference's overload)."""
     r = C.c_double()
-    _c(x.system.lib.c2q_squarenorm(x.h, C.byref(r)), x)
+    if isinstance(x, Gaugemomenta):
+        _c(x.system.lib.c2q_gaugemomenta_squarenorm(x.h, C.byref(r)), x)
+    else:
+        _c(x.system.lib.c2q_squarenorm(x.h, C.byref(r)), x)
     return r.value
 
 
@@ -711,3 +718,95 @@ def request_footprint(lattice: Lattice, nsrc: int, precision: int = 16) -> int:
     """Device bytes a serving request holds while it runs (its admission footprint)."""
     lc = lattice.c()
     return L.load().c2q_request_footprint(C.byref(lc), nsrc, precision)
+
+
+# ---------------- HMC callers of the eo solvers ----------------
+class Gaugemomenta:
+    """physics::lattices::Gaugemomenta: 8 reals (the su(3) algebra element) per
+    link; host format ae[4V] at link mu + 4 site."""
+
+    def __init__(self, system: System, lattice: Lattice, aos: np.ndarray | None = None):
+        self.system, self.lattice = system, lattice
+        lib = system.lib
+        h = C.c_void_p()
+        lc = lattice.c()
+        _check(lib.c2q_gaugemomenta_create(system.h, C.byref(lc), C.byref(h)), system.h, lib)
+        self.h = h
+        system._adopt(self)
+        if aos is not None:
+            self.upload(aos)
+
+    def zero(self):
+        _c(self.system.lib.c2q_gaugemomenta_zero(self.h), self)
+
+    def upload(self, aos):
+        aos = np.ascontiguousarray(aos, dtype=np.float64)
+        assert aos.size == 4 * self.lattice.vol * 8
+        _c(self.system.lib.c2q_gaugemomenta_upload(self.h, aos.reshape(-1)), self)
+
+    def download(self):
+        out = np.zeros(4 * self.lattice.vol * 8)
+        _c(self.system.lib.c2q_gaugemomenta_download(self.h, out), self)
+        return out.reshape(4 * self.lattice.vol, 8)
+
+    def _destroy(self):
+        if getattr(self, "h", None) and getattr(self.system, "h", None):
+            self.system.lib.c2q_gaugemomenta_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        try:
+            self._destroy()
+        except Exception:
+            pass
+
+
+def fermion_force(gm: Gaugemomenta, Y, X, evenodd: int, gf: Gaugefield, add: AdditionalParameters):
+    """physics::algorithms::fermion_force on eo fields (fermion_force.cpp:699-730):
+    gm += the force of Y (on the sites evenodd selects: ODD the even ones) and X."""
+    _c(gm.system.lib.c2q_fermion_force_eo(gm.h, gf.h, Y.h, X.h, evenodd, add.kappa), gm)
+
+
+def _odd_partner(out, tmp, gf, field, add, action, minus):
+    """out = -M^-1 D(ODD) field (tm; -D(ODD) field for Wilson), fermion_force.cpp:144-175."""
+    dslash(out, gf, field, ODD, add.kappa)
+    if action == "twistedmass":
+        (M_tm_inverse_sitediagonal_minus if minus else M_tm_inverse_sitediagonal)(tmp, out, add.mubar)
+        sax(out, -1.0, tmp)
+    else:
+        sax(out, -1.0, out)
+
+
+def calc_fermion_force(force: Gaugemomenta, gf: Gaugefield, phi, params: SolverParameters,
+                       add: AdditionalParameters, action: str = "twistedmass", report: dict | None = None) -> int:
+    """physics::algorithms::calc_fermion_force on eo fields, CG branch
+    (fermion_force.cpp:37-80, 131-175): X = (Q+Q-)^-1 phi from a cold start,
+    Y = Q- X, force += F(Y, X_odd, EVEN) + F(Y_odd, X, ODD).  The solve takes
+    `params` (FP64 with the reference's semantics, or the mixed-precision CG).
+    Returns the CG's iteration count."""
+    system, lat = phi.system, phi.lattice
+    x = Spinorfield_eo(system, lat)
+    y = Spinorfield_eo(system, lat)
+    tmp1 = Spinorfield_eo(system, lat)
+    tmp2 = Spinorfield_eo(system, lat)
+    x.cold()
+    it = cg(x, QplusQminus_eo(action), gf, phi, params, add, report)
+    Qminus_eo(action)(y, gf, x, add)
+    _odd_partner(tmp1, tmp2, gf, x, add, action, minus=True)
+    fermion_force(force, y, tmp1, EVEN, gf, add)
+    _odd_partner(tmp1, tmp2, gf, y, add, action, minus=False)
+    fermion_force(force, tmp1, x, ODD, gf, add)
+    return it
+
+
+def calc_s_fermion(gf: Gaugefield, phi, params: SolverParameters, add: AdditionalParameters,
+                   action: str = "twistedmass", report: dict | None = None) -> float:
+    """physics::algorithms::calc_s_fermion on eo fields, CG branch (metropolis.cpp:79-121):
+    X = (Q+Q-)^-1 phi from a cold start, S_f = |Q- X|^2."""
+    system, lat = phi.system, phi.lattice
+    x = Spinorfield_eo(system, lat)
+    y = Spinorfield_eo(system, lat)
+    x.cold()
+    cg(x, QplusQminus_eo(action), gf, phi, params, add, report)
+    Qminus_eo(action)(y, gf, x, add)
+    return squarenorm(y)

@@ -319,6 +319,27 @@ C2Q_EXPORT int c2q_perform_inversion_eo_fields(c2q_ctx* ctx, c2q_spinor_eo* out_
 C2Q_EXPORT int c2q_correlator_ps(const c2q_spinor_eo* const* even, const c2q_spinor_eo* const* odd, int n,
                                  double kappa, int direction, double* out);
 
+/* ---------------- HMC callers of the eo solvers ----------------
+ * Gauge momenta (physics::lattices::Gaugemomenta, physics/lattices/gaugemomenta.hpp):
+ * 8 reals (the su(3) algebra element ae, common_header_files/types.hpp:178-188)
+ * per link; host format ae[4 V] at link mu + 4 site, TDIR = 0. */
+typedef struct c2q_gaugemomenta c2q_gaugemomenta;
+C2Q_EXPORT int c2q_gaugemomenta_create(c2q_ctx* ctx, const c2q_lattice* lat, c2q_gaugemomenta** out);
+C2Q_EXPORT int c2q_gaugemomenta_destroy(c2q_gaugemomenta* gm);
+/* Gaugemomenta::zero (gaugemomentum_zero.cl) */
+C2Q_EXPORT int c2q_gaugemomenta_zero(c2q_gaugemomenta* gm);
+C2Q_EXPORT int c2q_gaugemomenta_upload(c2q_gaugemomenta* gm, const double* aos);
+C2Q_EXPORT int c2q_gaugemomenta_download(const c2q_gaugemomenta* gm, double* aos);
+/* squarenorm(const Gaugemomenta&) (gaugemomentum_squarenorm.cl): sum of e_k^2 over every link */
+C2Q_EXPORT int c2q_gaugemomenta_squarenorm(const c2q_gaugemomenta* gm, double* out);
+/* physics::algorithms::fermion_force(gm, Y, X, evenodd, gf, params) on eo fields
+ * (physics/algorithms/fermion_force.cpp:699-730; kernels fermion_force_eo_0..3,
+ * ocl_kernel/force_fermion_eo.cl, via hardware/code/molecular_dynamics.cpp:543-625):
+ * gm += the force of Y on the sites evenodd selects (C2Q_ODD: x+y+z+t even) and X
+ * on the other parity; FP64. */
+C2Q_EXPORT int c2q_fermion_force_eo(c2q_gaugemomenta* gm, const c2q_gauge* g, const c2q_spinor_eo* Y,
+                                    const c2q_spinor_eo* X, int evenodd, double kappa);
+
 /* ---------------- inputs ---------------- */
 /* Seeded synthetic gauge field U = exp(i eps H), H traceless Hermitian with
  * N(0,1) entries, reunitarised in FP64 (host computation, no GPU needed).

@@ -99,6 +99,10 @@ class Oracle:
             "c2qo_cg": (i, [_D, i, _D, _D, d, d, i, C.POINTER(SolverParams)]),
             "c2qo_bicgstab": (i, [_D, i, _D, _D, d, d, i, C.POINTER(SolverParams)]),
             "c2qo_perform_inversion_eo": (i, [_D, _D, _D, d, d, i, C.POINTER(SolverParams), C.POINTER(i)]),
+            "c2qo_fermion_force_eo": (None, [_D, _D, _D, _D, i, d]),
+            "c2qo_gm_squarenorm": (d, [_D]),
+            "c2qo_calc_fermion_force_eo": (i, [_D, _D, _D, d, d, i, C.POINTER(SolverParams)]),
+            "c2qo_calc_s_fermion_eo": (d, [_D, _D, d, d, i, C.POINTER(SolverParams), C.POINTER(i)]),
             "c2qo_pseudo_randomize": (None, [_D, sz, i]),
             "c2qo_fill_gauge": (None, [_D, sz, i]),
             "c2qo_fill_ascending_complex": (None, [_D, sz]),
@@ -235,6 +239,28 @@ class Oracle:
         return out, it, bool(used.value)
 
     # ---- reference test fills ----
+    # ---- HMC callers (gauge momenta: ae[4V], link mu + 4 site, 8 doubles) ----
+    def gm_field(self):
+        return np.zeros((4 * self.vol, 8))
+
+    def fermion_force_eo(self, gm, Y, X, gauge, evenodd, kappa):
+        """gm += the eo fermion force (in place)."""
+        self.lib.c2qo_fermion_force_eo(gm, Y, X, gauge, evenodd, kappa)
+        return gm
+
+    def gm_squarenorm(self, gm):
+        return self.lib.c2qo_gm_squarenorm(gm)
+
+    def calc_fermion_force_eo(self, gm, phi, gauge, kappa, mubar, action=TWISTEDMASS, params=None):
+        params = params or SolverParams()
+        return self.lib.c2qo_calc_fermion_force_eo(gm, phi, gauge, kappa, mubar, action, C.byref(params))
+
+    def calc_s_fermion_eo(self, phi, gauge, kappa, mubar, action=TWISTEDMASS, params=None):
+        params = params or SolverParams()
+        it = C.c_int(0)
+        s = self.lib.c2qo_calc_s_fermion_eo(phi, gauge, kappa, mubar, action, C.byref(params), C.byref(it))
+        return s, it.value
+
     def pseudo_randomize(self, n_sites, seed):
         a = np.zeros((n_sites, 24))
         self.lib.c2qo_pseudo_randomize(a, a.size, seed)

@@ -389,6 +389,77 @@ C2QO_API int c2qo_bicgstab(double* x, int op, const double* b, const double* g, 
     return P->solver == 3 ? bicgstab_save(x, &A, b, P) : bicgstab_fast(x, &A, b, P);
 }
 
+/* ------------------------------ HMC callers ------------------------------ */
+/* physics::algorithms::fermion_force(gm, Y, X, evenodd, ...) on the eo fields
+ * (fermion_force.cpp:699-730 -> molecular_dynamics.cpp:543-625) */
+C2QO_API void c2qo_fermion_force_eo(double* gm, const double* Y, const double* X, const double* g, int evenodd,
+                                    double kappa)
+{
+    ok_fermion_force_eo(gm, Y, X, g, evenodd, kappa);
+}
+
+/* squarenorm of gauge momenta ae[4V] (gaugemomentum_squarenorm.cl: the sum of
+ * e_k^2 over every link) */
+C2QO_API double c2qo_gm_squarenorm(const double* gm)
+{
+    const size_t n = 4 * 8 * ok_vol();
+    double s       = 0.;
+    for (size_t k = 0; k < n; ++k) s += gm[k] * gm[k];
+    return s;
+}
+
+/* calc_fermion_force on eo fields, CG branch (fermion_force.cpp:37-80, 131-175):
+ * X = (Q+Q-)^-1 phi from a cold start, Y = Q- X, then
+ *   X_odd = -M^-1_minus D(ODD) X,  F += F(Y, X_odd, EVEN),
+ *   Y_odd = -M^-1 D(ODD) Y,        F += F(Y_odd, X, ODD)
+ * (Wilson: the site-diagonal inverse is 1).  Returns the CG's iteration count. */
+C2QO_API int c2qo_calc_fermion_force_eo(double* gm, const double* phi, const double* g, double kappa, double mubar,
+                                        int action, const c2qo_solver_params* P)
+{
+    double *x = field_alloc(), *y = field_alloc(), *tmp1 = field_alloc(), *tmp2 = field_alloc();
+    ok_cold(x);
+    const int it = c2qo_cg(x, C2QO_OP_QPQM_EO, phi, g, kappa, mubar, action, P);
+    c2qo_apply(C2QO_OP_QMINUS_EO, y, x, g, kappa, mubar, action, P->merge_fermion);
+    const c2qo_complex m1 = {-1., 0.};
+    ok_dslash_eo(tmp1, x, g, 1 /*ODD*/, kappa);
+    if (action == C2QO_TWISTEDMASS) {
+        ok_tm_diag(tmp2, tmp1, mubar, C2QO_DIAG_MINV_MINUS);
+        ok_sax(tmp1, m1, tmp2);
+    } else {
+        ok_sax(tmp1, m1, tmp1);
+    }
+    ok_fermion_force_eo(gm, y, tmp1, g, 0 /*EVEN*/, kappa);
+    ok_dslash_eo(tmp1, y, g, 1 /*ODD*/, kappa);
+    if (action == C2QO_TWISTEDMASS) {
+        ok_tm_diag(tmp2, tmp1, mubar, C2QO_DIAG_MINV);
+        ok_sax(tmp1, m1, tmp2);
+    } else {
+        ok_sax(tmp1, m1, tmp1);
+    }
+    ok_fermion_force_eo(gm, tmp1, x, g, 1 /*ODD*/, kappa);
+    free(x);
+    free(y);
+    free(tmp1);
+    free(tmp2);
+    return it;
+}
+
+/* calc_s_fermion on eo fields, CG branch (metropolis.cpp:79-121): X = (Q+Q-)^-1
+ * phi from a cold start, S_f = |Q- X|^2.  *iters receives the CG's count. */
+C2QO_API double c2qo_calc_s_fermion_eo(const double* phi, const double* g, double kappa, double mubar, int action,
+                                       const c2qo_solver_params* P, int* iters)
+{
+    double *x = field_alloc(), *y = field_alloc();
+    ok_cold(x);
+    const int it = c2qo_cg(x, C2QO_OP_QPQM_EO, phi, g, kappa, mubar, action, P);
+    if (iters) *iters = it;
+    c2qo_apply(C2QO_OP_QMINUS_EO, y, x, g, kappa, mubar, action, P->merge_fermion);
+    const double s2 = ok_squarenorm(y);
+    free(x);
+    free(y);
+    return s2;
+}
+
 /* Eo branch of invert_M_nf2_upperflavour, inversion.cpp:129-236, including the
  * parity-role swap (issue #387 workaround, :141-149) and the sign convention of
  * the prepared source and the odd reconstruction (:165-169, :204-221).

@@ -74,6 +74,11 @@ void ok_m_tm_minus(double* out, const double* in, const double* gauge, double ka
 void ok_gamma5_full(double* inout);
 double ok_squarenorm_full(const double* x);
 
+/* fermion_force_eo_0..3 (ocl_kernel/force_fermion_eo.cl): gm (ae[4V], link
+ * mu + 4*site, 8 doubles) += the eo fermion force of Y (on the sites evenodd
+ * selects: ODD the even ones) and X (the other parity). */
+void ok_fermion_force_eo(double* gm, const double* Y, const double* X, const double* gauge, int evenodd, double kappa);
+
 /* Name of the backend ("port" or "reference"). */
 const char* ok_backend_name(void);
 

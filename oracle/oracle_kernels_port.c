@@ -46,6 +46,10 @@
 static c2qo_lattice g_lat = {4, 4, 0., 0., 0, 0, 0., 0.};
 /* hop coefficients: [dir][0 = forward, 1 = backward] as (re, im) */
 static double g_hop[4][2][2];
+/* the plain boundary phase e^{i theta pi / N} per direction, and the chemical
+ * potential factors of the T link in the fermion force (forward, backward) */
+static double g_phase[4][2];
+static double g_cp_link[2][2];
 
 static double as_build_option(double v)
 {
@@ -64,6 +68,19 @@ void ok_set_lattice(const c2qo_lattice* lat)
         g_hop[mu][0][1] = s;
         g_hop[mu][1][0] = c;
         g_hop[mu][1][1] = -s;
+        g_phase[mu][0]  = c;
+        g_phase[mu][1]  = s;
+    }
+    {
+        /* hardware/code/opencl_module.cpp:113-124: EXPCPR, MEXPCPR, COSCPI, SINCPI */
+        const double er  = lat->use_cp_re ? as_build_option(exp(lat->cp_re)) : 1.;
+        const double emr = lat->use_cp_re ? as_build_option(exp(-lat->cp_re)) : 1.;
+        const double cc  = lat->use_cp_im ? as_build_option(cos(lat->cp_im)) : 1.;
+        const double ss  = lat->use_cp_im ? as_build_option(sin(lat->cp_im)) : 0.;
+        g_cp_link[0][0] = er * cc;
+        g_cp_link[0][1] = er * ss;
+        g_cp_link[1][0] = emr * cc;
+        g_cp_link[1][1] = emr * ss;
     }
     if (lat->use_cp_re || lat->use_cp_im) {
         double er = lat->use_cp_re ? exp(lat->cp_re) : 1., emr = lat->use_cp_re ? exp(-lat->cp_re) : 1.;
@@ -402,4 +419,85 @@ void ok_m_tm_plus(double* out, const double* in, const double* gauge, double kap
 void ok_m_tm_minus(double* out, const double* in, const double* gauge, double kappa, double mubar)
 {
     m_tm_full(out, in, gauge, kappa, mubar, 1);
+}
+
+/* ---------------- fermion force (eo) ----------------
+ * The four kernels fermion_force_eo_0..3 (ocl_kernel/force_fermion_eo.cl:31-459)
+ * in one pass.  At every site x of the parity selected by evenodd (ODD = 1: the
+ * even sites, as get_even_st_idx; EVEN = 0: the odd ones) with y = g5 Y(x):
+ *   forward hop : the upper rows a, b of phi = (1 - g_mu) y and of
+ *                 psi = (1 - g_mu) X(x + mu) give v = phi_a psi_a^+ + phi_b psi_b^+
+ *                 (tr_v_times_u_dagger, operations_su3vec.cl:228-250) and
+ *                 F(x, mu) += tr_lambda(bc_mu U_mu(x) v^+);
+ *   backward hop: with (1 + g_mu) and X(x - mu), v = psi_a phi_a^+ + psi_b phi_b^+
+ *                 and F(x - mu, mu) += tr_lambda(bc_mu U_mu(x - mu) v^+);
+ * bc_mu = 2 kappa e^{i theta pi / N} for both hops; on T links U is multiplied by
+ * e^{cp_re} e^{i cp_im} (forward) or e^{-cp_re} e^{i cp_im} (backward).
+ * tr_lambda(M)_k = Tr[i T_k (M - M^+)] with T_k = lambda_k / 2
+ * (tr_lambda_u, operations_gaugemomentum.cl:68-88, including its 1/sqrt(3)
+ * literal).  Gauge momenta: ae[4 V] at link mu + 4 site, 8 doubles each.  Every
+ * link gets at most one contribution per call, so the site loop is parallel. */
+static void tr_lambda(const cplx M[9], double ae[8])
+{
+    ae[0] = -M[3].i - M[1].i;
+    ae[1] = M[3].r - M[1].r;
+    ae[2] = -M[0].i + M[4].i;
+    ae[3] = -M[6].i - M[2].i;
+    ae[4] = M[6].r - M[2].r;
+    ae[5] = -M[7].i - M[5].i;
+    ae[6] = M[7].r - M[5].r;
+    ae[7] = (-M[0].i - M[4].i + 2.0 * M[8].i) * 0.577350269189625;
+}
+
+void ok_fermion_force_eo(double* gm, const double* Y, const double* X, const double* gauge, int evenodd, double kappa)
+{
+    const int par = evenodd == 1 ? 0 : 1;
+    const long n  = (long)ok_seo();
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; ++i) {
+        const size_t s = eo_site((size_t)i, par);
+        double y[24];
+        for (int k = 0; k < 24; ++k) y[k] = k < 12 ? Y[24 * i + k] : -Y[24 * i + k];
+        for (int mu = 0; mu < 4; ++mu) {
+            const cplx bc = {2. * kappa * g_phase[mu][0], 2. * kappa * g_phase[mu][1]};
+            for (int back = 0; back < 2; ++back) {
+                const size_t sn    = shift_site(s, mu, back ? -1 : +1);
+                const size_t ls    = back ? sn : s; /* the link's site */
+                const double* plus = X + 24 * (sn / 2);
+                cplx U[9];
+                for (int e = 0; e < 9; ++e) {
+                    U[e] = cld(gauge + 18 * (mu + 4 * ls) + 2 * e);
+                    if (mu == 0) U[e] = cmul(U[e], (cplx){g_cp_link[back][0], g_cp_link[back][1]});
+                }
+                cplx psi[2][3], phi[2][3];
+                for (int a = 0; a < 2; ++a) {
+                    const int p = PROJ_P[mu][a];
+                    cplx c      = {PROJ_C[mu][a][0], PROJ_C[mu][a][1]};
+                    if (back) c = (cplx){-c.r, -c.i};
+                    for (int col = 0; col < 3; ++col) {
+                        psi[a][col] = cadd(cld(plus + 6 * a + 2 * col), cmul(c, cld(plus + 6 * p + 2 * col)));
+                        phi[a][col] = cadd(cld(y + 6 * a + 2 * col), cmul(c, cld(y + 6 * p + 2 * col)));
+                    }
+                }
+                cplx v[9], w[9];
+                for (int r = 0; r < 3; ++r)
+                    for (int q = 0; q < 3; ++q) {
+                        cplx acc = {0., 0.};
+                        for (int a = 0; a < 2; ++a)
+                            acc = cadd(acc, back ? cmul(psi[a][r], cconj(phi[a][q])) : cmul(phi[a][r], cconj(psi[a][q])));
+                        v[3 * r + q] = acc;
+                    }
+                for (int r = 0; r < 3; ++r)
+                    for (int q = 0; q < 3; ++q) {
+                        cplx acc = {0., 0.};
+                        for (int k = 0; k < 3; ++k) acc = cadd(acc, cmul(U[3 * r + k], cconj(v[3 * q + k])));
+                        w[3 * r + q] = cmul(acc, bc);
+                    }
+                double ae[8];
+                tr_lambda(w, ae);
+                double* dst = gm + 8 * (mu + 4 * ls);
+                for (int k = 0; k < 8; ++k) dst[k] += ae[k];
+            }
+        }
+    }
 }

@@ -66,6 +66,8 @@ double c2qref_expcpr = 1., c2qref_mexpcpr = 1., c2qref_coscpi = 1., c2qref_sincp
 #include "ocl_kernel/spinorfield_eo_zero.cl"
 #include "ocl_kernel/spinorfield_eo_cold.cl"
 #include "ocl_kernel/spinorfield_eo_convert.cl"
+#include "ocl_kernel/operations_gaugemomentum.cl"
+#include "ocl_kernel/force_fermion_eo.cl"
 
 #include "oracle_kernels.h"
 
@@ -267,3 +269,13 @@ void ok_m_tm_minus(double* out, const double* in, const double* gauge, double ka
 }
 
 void ok_gamma5_full(double* inout) { LAUNCH(gamma5((spinor*)inout)); }
+
+/* hardware/code/molecular_dynamics.cpp:543-625 fermion_force_eo_device: the four
+ * direction kernels one after the other on the same momenta */
+void ok_fermion_force_eo(double* gm, const double* Y, const double* X, const double* gauge, int evenodd, double kappa)
+{
+    LAUNCH(fermion_force_eo_0((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, evenodd, kappa));
+    LAUNCH(fermion_force_eo_1((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, evenodd, kappa));
+    LAUNCH(fermion_force_eo_2((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, evenodd, kappa));
+    LAUNCH(fermion_force_eo_3((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, evenodd, kappa));
+}

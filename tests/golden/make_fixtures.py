@@ -8,6 +8,8 @@ reference tree and the oracle built; the fixtures themselves are committed).
      cold 4^3x16 block, seeds 5..9);
    * physics/fermionmatrix/explicit_test.cpp: dslash (seed 13) and the four
      M_tm_*sitediagonal* cases (seeds 5, 7, 9, 11);
+   * physics/algorithms/fermion_force_test.cpp: the eo fermion force (squarenorm
+     of the momenta, cold 4^3x16 and conf.00200);
    * hardware/code/fermions_test.cpp: the closed form of the dslash_eo
      kernel test in theta and the chemical potential, and the
      M_tm_sitediagonal family per-site constants.
@@ -114,6 +116,19 @@ def extract_kats(ref: str) -> dict:
                                                "refs": [float(r) for r in refs[:2]], "operator": fn[0],
                                                "kappa": 0.125, "mu": 0.006, "lattice": [4, 4],
                                                "where": "physics/fermionmatrix/explicit_test.cpp"}
+    # physics/algorithms/fermion_force_test.cpp, case fermion_force_eo: squarenorm of the
+    # momenta after F(sf1, sf2, EVEN) and after adding F(sf1, sf2, ODD), with sf1, sf2 the
+    # eo halves of a drand48 full field; cold 4^3x16 and conf.00200 (4^4), kappa .125
+    ff = open(os.path.join(ref, "physics/algorithms/fermion_force_test.cpp")).read()
+    m = re.search(r"BOOST_AUTO_TEST_CASE\(fermion_force_eo\)(.*?)(?=BOOST_AUTO_TEST_CASE|\Z)", ff, re.S)
+    out["fermion_force_eo"] = []
+    for blk in m.group(1).split("using namespace physics::lattices;")[1:]:
+        nt = re.findall(r"--nTime=(\d+)", blk)
+        seed = re.findall(r"pseudo_randomize<Spinorfield, spinor>\(&src, (\d+)\)", blk)
+        refs = re.findall(r"BOOST_CHECK_CLOSE\(squarenorm\(gm\), ([-+0-9.eE]+), 0\.01\)", blk)
+        out["fermion_force_eo"].append({"nt": int(nt[0]), "gauge": "conf.00200" if "conf.00200" in blk else "cold",
+                                        "seed": int(seed[0]), "refs": [float(r) for r in refs], "kappa": 0.125,
+                                        "where": "physics/algorithms/fermion_force_test.cpp"})
     # integration references of the inverter executable (executables/tests/testInverter.py:
     # the pseudoscalar correlator lines, compared at 0.1 %), with their input files
     out["inverter"] = {}
