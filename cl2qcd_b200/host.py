@@ -761,10 +761,20 @@ class Gaugemomenta:
             pass
 
 
-def fermion_force(gm: Gaugemomenta, Y, X, evenodd: int, gf: Gaugefield, add: AdditionalParameters):
-    """physics::algorithms::fermion_force on eo fields (fermion_force.cpp:699-730):
-    gm += the force of Y (on the sites evenodd selects: ODD the even ones) and X."""
-    _c(gm.system.lib.c2q_fermion_force_eo(gm.h, gf.h, Y.h, X.h, evenodd, add.kappa), gm)
+def fermion_force(gm: Gaugemomenta, Y, X, *args):
+    """physics::algorithms::fermion_force, both overloads:
+    fermion_force(gm, Y, X, evenodd, gf, add) on eo fields (fermion_force.cpp:699-730):
+    gm += the force of Y (on the sites evenodd selects: ODD the even ones) and X;
+    fermion_force(gm, Y, X, gf, add) on full fields (fermion_force.cpp:672-697,
+    force_fermion.cl): the same sum over every site, i.e. the eo force of both parities."""
+    lib = gm.system.lib
+    if isinstance(Y, Spinorfield):
+        gf, add = args
+        _c(lib.c2q_fermion_force_eo(gm.h, gf.h, Y.even.h, X.odd.h, ODD, add.kappa), gm)
+        _c(lib.c2q_fermion_force_eo(gm.h, gf.h, Y.odd.h, X.even.h, EVEN, add.kappa), gm)
+    else:
+        evenodd, gf, add = args
+        _c(lib.c2q_fermion_force_eo(gm.h, gf.h, Y.h, X.h, evenodd, add.kappa), gm)
 
 
 def _odd_partner(out, tmp, gf, field, add, action, minus):

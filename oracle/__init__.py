@@ -101,6 +101,7 @@ class Oracle:
             "c2qo_perform_inversion_eo": (i, [_D, _D, _D, d, d, i, C.POINTER(SolverParams), C.POINTER(i)]),
             "c2qo_fermion_force_eo": (None, [_D, _D, _D, _D, i, d]),
             "c2qo_gm_squarenorm": (d, [_D]),
+            "c2qo_fermion_force_full": (None, [_D, _D, _D, _D, d]),
             "c2qo_calc_fermion_force_eo": (i, [_D, _D, _D, d, d, i, C.POINTER(SolverParams)]),
             "c2qo_calc_s_fermion_eo": (d, [_D, _D, d, d, i, C.POINTER(SolverParams), C.POINTER(i)]),
             "c2qo_pseudo_randomize": (None, [_D, sz, i]),
@@ -246,6 +247,11 @@ class Oracle:
     def fermion_force_eo(self, gm, Y, X, gauge, evenodd, kappa):
         """gm += the eo fermion force (in place)."""
         self.lib.c2qo_fermion_force_eo(gm, Y, X, gauge, evenodd, kappa)
+        return gm
+
+    def fermion_force_full(self, gm, Y, X, gauge, kappa):
+        """gm += the non-eo fermion force of full fields Y, X (in place)."""
+        self.lib.c2qo_fermion_force_full(gm, Y, X, gauge, kappa)
         return gm
 
     def gm_squarenorm(self, gm):

@@ -398,6 +398,13 @@ C2QO_API void c2qo_fermion_force_eo(double* gm, const double* Y, const double* X
     ok_fermion_force_eo(gm, Y, X, g, evenodd, kappa);
 }
 
+/* physics::algorithms::fermion_force(gm, Y, X, ...) on full fields
+ * (fermion_force.cpp:672-697 -> force_fermion.cl) */
+C2QO_API void c2qo_fermion_force_full(double* gm, const double* Y, const double* X, const double* g, double kappa)
+{
+    ok_fermion_force_full(gm, Y, X, g, kappa);
+}
+
 /* squarenorm of gauge momenta ae[4V] (gaugemomentum_squarenorm.cl: the sum of
  * e_k^2 over every link) */
 C2QO_API double c2qo_gm_squarenorm(const double* gm)

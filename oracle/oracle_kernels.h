@@ -78,6 +78,8 @@ double ok_squarenorm_full(const double* x);
  * mu + 4*site, 8 doubles) += the eo fermion force of Y (on the sites evenodd
  * selects: ODD the even ones) and X (the other parity). */
 void ok_fermion_force_eo(double* gm, const double* Y, const double* X, const double* gauge, int evenodd, double kappa);
+/* fermion_force (ocl_kernel/force_fermion.cl): the same on full fields spinor[V]. */
+void ok_fermion_force_full(double* gm, const double* Y, const double* X, const double* gauge, double kappa);
 
 /* Name of the backend ("port" or "reference"). */
 const char* ok_backend_name(void);

@@ -501,3 +501,22 @@ void ok_fermion_force_eo(double* gm, const double* Y, const double* X, const dou
         }
     }
 }
+
+/* the non-eo force (ocl_kernel/force_fermion.cl) sums the same two hops over
+ * every site: the eo force of the even sites plus that of the odd ones */
+void ok_fermion_force_full(double* gm, const double* Y, const double* X, const double* gauge, double kappa)
+{
+    const size_t seo = ok_seo();
+    double* ye       = malloc(24 * seo * sizeof(double));
+    double* yo       = malloc(24 * seo * sizeof(double));
+    double* xe       = malloc(24 * seo * sizeof(double));
+    double* xo       = malloc(24 * seo * sizeof(double));
+    ok_convert_to_eo(ye, yo, Y);
+    ok_convert_to_eo(xe, xo, X);
+    ok_fermion_force_eo(gm, ye, xo, gauge, 1 /*ODD: the even sites*/, kappa);
+    ok_fermion_force_eo(gm, yo, xe, gauge, 0 /*EVEN: the odd sites*/, kappa);
+    free(ye);
+    free(yo);
+    free(xe);
+    free(xo);
+}

@@ -68,6 +68,7 @@ double c2qref_expcpr = 1., c2qref_mexpcpr = 1., c2qref_coscpi = 1., c2qref_sincp
 #include "ocl_kernel/spinorfield_eo_convert.cl"
 #include "ocl_kernel/operations_gaugemomentum.cl"
 #include "ocl_kernel/force_fermion_eo.cl"
+#include "ocl_kernel/force_fermion.cl"
 
 #include "oracle_kernels.h"
 
@@ -278,4 +279,10 @@ void ok_fermion_force_eo(double* gm, const double* Y, const double* X, const dou
     LAUNCH(fermion_force_eo_1((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, evenodd, kappa));
     LAUNCH(fermion_force_eo_2((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, evenodd, kappa));
     LAUNCH(fermion_force_eo_3((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, evenodd, kappa));
+}
+
+/* molecular_dynamics.cpp fermion_force_device: the non-eo kernel on full fields */
+void ok_fermion_force_full(double* gm, const double* Y, const double* X, const double* gauge, double kappa)
+{
+    LAUNCH(fermion_force((const Matrixsu3*)gauge, (const spinor*)Y, (const spinor*)X, (ae*)gm, kappa));
 }

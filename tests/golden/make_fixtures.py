@@ -129,6 +129,16 @@ def extract_kats(ref: str) -> dict:
         out["fermion_force_eo"].append({"nt": int(nt[0]), "gauge": "conf.00200" if "conf.00200" in blk else "cold",
                                         "seed": int(seed[0]), "refs": [float(r) for r in refs], "kappa": 0.125,
                                         "where": "physics/algorithms/fermion_force_test.cpp"})
+    # the same file, case fermion_force: the non-eo force of two drand48 full fields
+    m = re.search(r"BOOST_AUTO_TEST_CASE\(fermion_force\)(.*?)(?=BOOST_AUTO_TEST_CASE|\Z)", ff, re.S)
+    out["fermion_force_full"] = []
+    for blk in m.group(1).split("using namespace physics::lattices;")[1:]:
+        nt = re.findall(r"--nTime=(\d+)", blk)
+        seeds = re.findall(r"pseudo_randomize<Spinorfield, spinor>\(&(sf\d), (\d+)\)", blk)
+        refs = re.findall(r"BOOST_CHECK_CLOSE\(squarenorm\(gm\), ([-+0-9.eE]+), 0\.01\)", blk)
+        out["fermion_force_full"].append({"nt": int(nt[0]), "gauge": "conf.00200" if "conf.00200" in blk else "cold",
+                                          "seeds": {k: int(v) for k, v in seeds}, "refs": [float(r) for r in refs],
+                                          "kappa": 0.125, "where": "physics/algorithms/fermion_force_test.cpp"})
     # integration references of the inverter executable (executables/tests/testInverter.py:
     # the pseudoscalar correlator lines, compared at 0.1 %), with their input files
     out["inverter"] = {}

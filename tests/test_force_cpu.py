@@ -44,6 +44,22 @@ def test_fermion_force_eo_kats(request, O, kind, case):
     assert both == pytest.approx(kat["refs"][1], rel=1e-10)
 
 
+@pytest.mark.parametrize("kind", ["port", "reference"])
+@pytest.mark.parametrize("case", range(len(KATS["fermion_force_full"])))
+def test_fermion_force_full_kats(request, O, kind, case):
+    """the non-eo force (case fermion_force): the reference's own kernel, and the
+    restatement as the eo force of both parities"""
+    o = _oracle(request, kind)
+    kat = KATS["fermion_force_full"][case]
+    o.set_lattice(4, kat["nt"])
+    g = CONF["gauge"] if kat["gauge"] == "conf.00200" else o.gauge_fill(False)
+    sf1 = o.pseudo_randomize(o.vol, kat["seeds"]["sf1"])
+    sf2 = o.pseudo_randomize(o.vol, kat["seeds"]["sf2"])
+    gm = o.gm_field()
+    o.fermion_force_full(gm, sf1, sf2, g, kat["kappa"])
+    assert o.gm_squarenorm(gm) == pytest.approx(kat["refs"][0], rel=1e-10)
+
+
 @pytest.mark.parametrize("bc", [(1.0, 0.0, None, None), (0.5, 0.3, None, 0.2), (1.0, 0.0, 0.1, None)])
 def test_force_port_matches_reference_kernel(port, ref, O, bc):
     tt, ts, cpr, cpi = bc

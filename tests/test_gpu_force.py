@@ -77,6 +77,22 @@ def test_fermion_force_kats(port, system, case):
     assert c2q.host.squarenorm(gm) == pytest.approx(kat["refs"][1], rel=1e-10)
 
 
+@pytest.mark.parametrize("case", range(len(KATS["fermion_force_full"])))
+def test_fermion_force_full_kats(port, system, case):
+    """the non-eo overload fermion_force(gm, Y, X, gf, params) on full fields"""
+    import cl2qcd_b200 as c2q
+    kat = KATS["fermion_force_full"][case]
+    port.set_lattice(4, kat["nt"])
+    L = c2q.Lattice(4, kat["nt"])
+    g = CONF["gauge"] if kat["gauge"] == "conf.00200" else port.gauge_fill(False)
+    gf = c2q.Gaugefield(system, L, g)
+    sf1 = c2q.host.Spinorfield(system, L, port.pseudo_randomize(port.vol, kat["seeds"]["sf1"]))
+    sf2 = c2q.host.Spinorfield(system, L, port.pseudo_randomize(port.vol, kat["seeds"]["sf2"]))
+    gm = c2q.host.Gaugemomenta(system, L)
+    c2q.host.fermion_force(gm, sf1, sf2, gf, c2q.AdditionalParameters(kat["kappa"], 0.0))
+    assert c2q.host.squarenorm(gm) == pytest.approx(kat["refs"][0], rel=1e-10)
+
+
 @pytest.mark.parametrize("precision", [64, 16])
 @pytest.mark.parametrize("action", ["twistedmass", "wilson"])
 def test_calc_fermion_force_and_energy(port, system, O, precision, action):
