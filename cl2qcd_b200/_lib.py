@@ -131,6 +131,12 @@ SIGNATURES = {
     "c2q_perform_inversion_eo_fields": (C.c_int, [_P, _P, _P, _P, _D, C.c_double, C.c_double, C.c_int,
                                                   C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
     "c2q_correlator_ps": (C.c_int, [C.POINTER(_P), C.POINTER(_P), C.c_int, C.c_double, C.c_int, _D]),
+    "c2q_cg_full": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, C.c_double, C.c_double, C.c_int,
+                              C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
+    "c2q_bicgstab_full": (C.c_int, [_P, _P, C.c_int, _P, _P, _P, C.c_double, C.c_double, C.c_int,
+                                    C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
+    "c2q_perform_inversion_full": (C.c_int, [_P, _D, _P, _D, C.c_double, C.c_double, C.c_int,
+                                             C.POINTER(CSolverParams), C.POINTER(CSolveReport)]),
     "c2q_gaugemomenta_create": (C.c_int, [_P, C.POINTER(CLattice), C.POINTER(_P)]),
     "c2q_gaugemomenta_destroy": (C.c_int, [_P]),
     "c2q_gaugemomenta_zero": (C.c_int, [_P]),

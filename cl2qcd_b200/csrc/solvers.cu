@@ -719,65 +719,162 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
     return n == 1 ? S[0].status : C2Q_OK;
 }
 
+// ------------------------------------------------- solver vector spaces
+// The vector space of a Krylov solve with host-side scalars: one FP64 eo field
+// (EoSpace), or a full field held as its two parities (FullSpace: the
+// reference's physics::lattices::Spinorfield of useEO=false inversions,
+// inversion.cpp:98-122).  Both provide the operator, the BLAS calls and the
+// inner products of the solvers; a full field's inner products are the sums of
+// its two halves'.
+struct EoSpace {
+    using V = c2q_spinor_eo*;
+    c2q_ctx* ctx;
+    const c2q_lattice* lat;
+    int op;
+    const c2q_gauge* g;
+    int gk;
+    double kappa, mubar;
+    int action;
+    Fields F;
+    c2q_spinor_eo *t1 = nullptr, *t2 = nullptr;
+    int sweeps = 0;
+    int alloc(int n, std::vector<V>& out)
+    {
+        int rc = make_fields(ctx, *lat, 64, n + 2, F, 0);
+        if (rc) return rc;
+        out.resize(n);
+        for (int k = 0; k < n; ++k) out[k] = &F.f[k];
+        t1 = &F.f[n];
+        t2 = &F.f[n + 1];
+        return C2Q_OK;
+    }
+    int apply(V out, V in)
+    {
+        return apply_operator(ctx, op, out, g, gk, in, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
+    }
+    int saxpy(V out, Cx a, V x, V y)
+    {
+        BlasSpec sp;
+        sp.op  = B_SAXPY;
+        sp.out = out;
+        sp.x   = x;
+        sp.y   = y;
+        sp.a   = coef_host(a.re, a.im);
+        return launch_blas(ctx, sp);
+    }
+    int saxsbypz(V out, Cx a, V x, Cx b, V y, V z)
+    {
+        BlasSpec sp;
+        sp.op  = B_SAXSBYPZ;
+        sp.out = out;
+        sp.x   = x;
+        sp.y   = y;
+        sp.z   = z;
+        sp.a   = coef_host(a.re, a.im);
+        sp.b   = coef_host(b.re, b.im);
+        return launch_blas(ctx, sp);
+    }
+    int copy(V to, V from) { return copy_field(ctx, to, from); }
+    int zero(V f) { return c2q_spinor_eo_zero(f); }
+    int dot(V x, V y, Cx* out) { return dot_read(ctx, x, y, out); }
+};
+
+struct FullSpace {
+    struct V {
+        c2q_spinor_eo *e, *o;  // the sites with x+y+z+t even, odd
+    };
+    c2q_ctx* ctx;
+    const c2q_lattice* lat;
+    int op;  // C2Q_FULL_*
+    const c2q_gauge* g;
+    double kappa, mubar;
+    int action;
+    Fields F;
+    EoSpace half;  // the BLAS of one parity (only its context is used)
+    int sweeps = 0;
+    int alloc(int n, std::vector<V>& out)
+    {
+        int rc = make_fields(ctx, *lat, 64, 2 * n, F, 0);
+        if (rc) return rc;
+        out.resize(n);
+        for (int k = 0; k < n; ++k) out[k] = V{&F.f[2 * k], &F.f[2 * k + 1]};
+        return C2Q_OK;
+    }
+    int apply(V out, V in)
+    {
+        sweeps += op == C2Q_FULL_QPLUSQMINUS ? 4 : 2;
+        return c2q_apply_full(op, out.e, out.o, g, in.e, in.o, kappa, mubar, action);
+    }
+    int saxpy(V out, Cx a, V x, V y)
+    {
+        int rc = half.saxpy(out.e, a, x.e, y.e);
+        return rc ? rc : half.saxpy(out.o, a, x.o, y.o);
+    }
+    int saxsbypz(V out, Cx a, V x, Cx b, V y, V z)
+    {
+        int rc = half.saxsbypz(out.e, a, x.e, b, y.e, z.e);
+        return rc ? rc : half.saxsbypz(out.o, a, x.o, b, y.o, z.o);
+    }
+    int copy(V to, V from)
+    {
+        int rc = copy_field(ctx, to.e, from.e);
+        return rc ? rc : copy_field(ctx, to.o, from.o);
+    }
+    int zero(V f)
+    {
+        int rc = c2q_spinor_eo_zero(f.e);
+        return rc ? rc : c2q_spinor_eo_zero(f.o);
+    }
+    int dot(V x, V y, Cx* out)
+    {
+        Cx a{0, 0}, b{0, 0};
+        int rc = dot_read(ctx, x.e, y.e, &a);
+        if (!rc) rc = dot_read(ctx, x.o, y.o, &b);
+        *out = {a.re + b.re, a.im + b.im};
+        return rc;
+    }
+};
+
 // ------------------------------------------------------------- BiCGStab
 // physics/algorithms/solvers/bicgstab.cpp:566-733 (fast) and :401-564 (save);
 // scalars are read back every iteration as the reference does.
-int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b,
-                  double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
+template <class S>
+int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_params* P, c2q_solve_report* rep)
 {
-    Fields F;
-    int rc = make_fields(ctx, x->lat, 64, 9, F, 0);
+    c2q_ctx* ctx = sp.ctx;
+    std::vector<typename S::V> w;
+    int rc = sp.alloc(7, w);
     if (rc) return rc;
-    c2q_spinor_eo *p = &F.f[0], *rn = &F.f[1], *rhat = &F.f[2], *s = &F.f[3], *t = &F.f[4], *v = &F.f[5],
-                  *aux = &F.f[6], *t1 = &F.f[7], *t2 = &F.f[8];
-    const int gk  = gkind_for(64, P->use_rec12);
+    const auto p = w[0], rn = w[1], rhat = w[2], s = w[3], t = w[4], v = w[5], aux = w[6];
     const bool save = P->solver == C2Q_SOLVER_BICGSTAB_SAVE;
-    int sweeps    = 0;
     SolveClock clock(ctx);
-    double b2 = 0;
-    rc        = saxpy_norm(ctx, aux, Cx{0, 0}, b, b, FIN_STORE_RESULT, &b2);
+    Cx bb{0, 0};
+    rc = sp.dot(b, b, &bb);
     if (rc) return rc;
+    const double b2  = bb.re;
     const double thr = stop_threshold(P, b2);
     const Cx one{1, 0}, mone{-1, 0};
     Cx alpha{1, 0}, omega{1, 0}, rho{1, 0}, rho_next, beta, tmp1, tmp2;
     double resid = std::numeric_limits<double>::quiet_NaN();
     int iter = 0, status = C2Q_DID_NOT_SOLVE;
 
-    auto apply = [&](c2q_spinor_eo* out, const c2q_spinor_eo* in) {
-        return apply_operator(ctx, op, out, g, gk, in, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
-    };
-    auto saxsbypz = [&](c2q_spinor_eo* out, Cx a, const c2q_spinor_eo* xx, Cx bb, const c2q_spinor_eo* yy,
-                        const c2q_spinor_eo* zz) {
-        BlasSpec sp;
-        sp.op  = B_SAXSBYPZ;
-        sp.out = out;
-        sp.x   = xx;
-        sp.y   = yy;
-        sp.z   = zz;
-        sp.a   = coef_host(a.re, a.im);
-        sp.b   = coef_host(bb.re, bb.im);
-        return launch_blas(ctx, sp);
-    };
-    auto saxpy = [&](c2q_spinor_eo* out, Cx a, const c2q_spinor_eo* xx, const c2q_spinor_eo* yy) {
-        BlasSpec sp;
-        sp.op  = B_SAXPY;
-        sp.out = out;
-        sp.x   = xx;
-        sp.y   = yy;
-        sp.a   = coef_host(a.re, a.im);
-        return launch_blas(ctx, sp);
-    };
-    auto sqnorm = [&](const c2q_spinor_eo* f, double* out) {
-        Cx c;
-        int r = dot_read(ctx, f, f, &c);
+    auto sqnorm = [&](typename S::V f, double* out) {
+        Cx c{0, 0};
+        int r = sp.dot(f, f, &c);
         *out  = c.re;
+        return r;
+    };
+    // true residual |b - A x|^2 into *tr (aux receives b - A x)
+    auto true_r2 = [&](double* tr) {
+        int r = sp.apply(aux, x);
+        if (!r) r = sp.saxpy(aux, one, aux, b);
+        if (!r) r = sqnorm(aux, tr);
         return r;
     };
     // true-residual confirmation (used by the save variant and by rel_tol)
     auto confirmed = [&](bool* ok) {
         double tr = 0;
-        int r     = apply(aux, x);
-        if (!r) r = saxpy_norm(ctx, aux, one, aux, b, FIN_STORE_RESULT, &tr);
+        int r     = true_r2(&tr);
         const double lim = P->rel_tol > 0 ? std::max(thr, 0.0) : P->prec;
         *ok              = tr < (P->rel_tol > 0 ? std::max(P->rel_tol * P->rel_tol * b2, P->prec > 0 ? P->prec : 0.0)
                                                  : lim);
@@ -787,11 +884,11 @@ int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, co
     if (!save) {
         for (iter = 0; iter < P->cgmax; iter++) {
             if (iter % P->iter_refresh == 0) {
-                rc = apply(rn, x);
-                if (!rc) rc = saxpy(p, one, rn, b);
-                if (!rc) rc = copy_field(ctx, rhat, p);
-                if (!rc) rc = copy_field(ctx, rn, p);
-                if (!rc) rc = dot_read(ctx, rhat, rn, &rho);
+                rc = sp.apply(rn, x);
+                if (!rc) rc = sp.saxpy(p, one, rn, b);
+                if (!rc) rc = sp.copy(rhat, p);
+                if (!rc) rc = sp.copy(rn, p);
+                if (!rc) rc = sp.dot(rhat, rn, &rho);
                 if (rc) return rc;
             }
             rc = sqnorm(rn, &resid);
@@ -811,19 +908,19 @@ int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, co
                     break;
                 }
             }
-            rc = apply(v, p);
-            if (!rc) rc = dot_read(ctx, rhat, v, &tmp1);
+            rc = sp.apply(v, p);
+            if (!rc) rc = sp.dot(rhat, v, &tmp1);
             if (rc) return rc;
             alpha = cdiv(rho, tmp1);
-            rc    = saxpy(s, alpha, v, rn);
-            if (!rc) rc = apply(t, s);
-            if (!rc) rc = dot_read(ctx, t, s, &tmp1);
-            if (!rc) rc = dot_read(ctx, t, t, &tmp2);
+            rc    = sp.saxpy(s, alpha, v, rn);
+            if (!rc) rc = sp.apply(t, s);
+            if (!rc) rc = sp.dot(t, s, &tmp1);
+            if (!rc) rc = sp.dot(t, t, &tmp2);
             if (rc) return rc;
             omega = cdiv(tmp1, tmp2);
-            rc    = saxsbypz(x, alpha, p, omega, s, x);
-            if (!rc) rc = saxpy(rn, omega, t, s);
-            if (!rc) rc = dot_read(ctx, rhat, rn, &rho_next);
+            rc    = sp.saxsbypz(x, alpha, p, omega, s, x);
+            if (!rc) rc = sp.saxpy(rn, omega, t, s);
+            if (!rc) rc = sp.dot(rhat, rn, &rho_next);
             if (rc) return rc;
             if (std::fabs(rho_next.re) < 1e-25 && std::fabs(rho_next.im) < 1e-25) {
                 status = C2Q_SOLVER_STUCK;
@@ -834,24 +931,24 @@ int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, co
             beta = cmulx(tmp1, tmp2);
             tmp1 = cmulx(beta, omega);
             tmp2 = cmulx(mone, tmp1);
-            rc   = saxsbypz(p, beta, p, tmp2, v, rn);
+            rc   = sp.saxsbypz(p, beta, p, tmp2, v, rn);
             if (rc) return rc;
             rho = rho_next;
         }
     } else {
         for (iter = 0; iter < P->cgmax; iter++) {
             if (iter % P->iter_refresh == 0) {
-                rc = c2q_spinor_eo_zero(v);
-                if (!rc) rc = c2q_spinor_eo_zero(p);
-                if (!rc) rc = apply(rn, x);
-                if (!rc) rc = saxpy(rn, one, rn, b);
-                if (!rc) rc = copy_field(ctx, rhat, rn);
+                rc = sp.zero(v);
+                if (!rc) rc = sp.zero(p);
+                if (!rc) rc = sp.apply(rn, x);
+                if (!rc) rc = sp.saxpy(rn, one, rn, b);
+                if (!rc) rc = sp.copy(rhat, rn);
                 if (rc) return rc;
                 alpha = one;
                 omega = one;
                 rho   = one;
             }
-            rc = dot_read(ctx, rhat, rn, &rho_next);
+            rc = sp.dot(rhat, rn, &rho_next);
             if (rc) return rc;
             if (std::fabs(rho_next.re) < 1e-25 && std::fabs(rho_next.im) < 1e-25) {
                 status = C2Q_SOLVER_STUCK;
@@ -863,19 +960,19 @@ int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, co
             beta = cmulx(tmp1, tmp2);
             tmp1 = cmulx(beta, omega);
             tmp2 = cmulx(mone, tmp1);
-            rc   = saxsbypz(p, beta, p, tmp2, v, rn);
-            if (!rc) rc = apply(v, p);
-            if (!rc) rc = dot_read(ctx, rhat, v, &tmp1);
+            rc   = sp.saxsbypz(p, beta, p, tmp2, v, rn);
+            if (!rc) rc = sp.apply(v, p);
+            if (!rc) rc = sp.dot(rhat, v, &tmp1);
             if (rc) return rc;
             alpha = cdiv(rho, tmp1);
-            rc    = saxpy(s, alpha, v, rn);
-            if (!rc) rc = apply(t, s);
-            if (!rc) rc = dot_read(ctx, t, s, &tmp1);
-            if (!rc) rc = dot_read(ctx, t, t, &tmp2);
+            rc    = sp.saxpy(s, alpha, v, rn);
+            if (!rc) rc = sp.apply(t, s);
+            if (!rc) rc = sp.dot(t, s, &tmp1);
+            if (!rc) rc = sp.dot(t, t, &tmp2);
             if (rc) return rc;
             omega = cdiv(tmp1, tmp2);
-            rc    = saxpy(rn, omega, t, s);
-            if (!rc) rc = saxsbypz(x, alpha, p, omega, s, x);
+            rc    = sp.saxpy(rn, omega, t, s);
+            if (!rc) rc = sp.saxsbypz(x, alpha, p, omega, s, x);
             if (!rc) rc = sqnorm(rn, &resid);
             if (rc) return rc;
             if (resid != resid) {
@@ -894,11 +991,100 @@ int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, co
         }
     }
     double r2t = 0;
-    rc         = true_residual(ctx, op, g, x, b, kappa, mubar, action, aux, t1, t2, &r2t, &sweeps);
+    rc         = true_r2(&r2t);
     if (rc) return rc;
-    finish_report(rep, status, iter, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sweeps);
+    finish_report(rep, status, iter, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sp.sweeps);
     if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
     if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "BiCGStab stuck (NaN residual or vanishing rho)");
+    return status;
+}
+
+int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b,
+                  double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
+{
+    EoSpace sp{ctx, &x->lat, op, g, gkind_for(64, P->use_rec12), kappa, mubar, action};
+    return bicgstab_generic(sp, x, const_cast<c2q_spinor_eo*>(b), P, rep);
+}
+
+// CG with host-side scalars, physics/algorithms/solvers/cg.cpp:277-400: the
+// residual is refreshed every iter_refresh iterations and checked every
+// resid_check_every (|r|^2 < prec; with rel_tol confirmed by the true
+// residual).  Used for the full-lattice solves of useEO=false inversions.
+template <class S>
+int cg_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_params* P, c2q_solve_report* rep)
+{
+    c2q_ctx* ctx = sp.ctx;
+    std::vector<typename S::V> w;
+    int rc = sp.alloc(4, w);
+    if (rc) return rc;
+    const auto p = w[0], rn = w[1], v = w[2], aux = w[3];
+    SolveClock clock(ctx);
+    Cx bb{0, 0};
+    rc = sp.dot(b, b, &bb);
+    if (rc) return rc;
+    const double b2  = bb.re;
+    const double thr = stop_threshold(P, b2);
+    const Cx one{1, 0};
+    Cx omega{0, 0}, rho{0, 0}, alpha{0, 0}, beta{0, 0}, omega_next{0, 0};
+    double resid = std::numeric_limits<double>::quiet_NaN();
+    int iter = 0, status = C2Q_DID_NOT_SOLVE;
+    bool force_refresh = false;
+    auto true_r2 = [&](double* tr) {
+        int r = sp.apply(aux, x);
+        if (!r) r = sp.saxpy(aux, one, aux, b);
+        Cx c{0, 0};
+        if (!r) r = sp.dot(aux, aux, &c);
+        *tr = c.re;
+        return r;
+    };
+    for (iter = 0; iter < P->cgmax || iter < P->min_iter; iter++) {
+        if (iter % P->iter_refresh == 0 || force_refresh) {
+            force_refresh = false;
+            rc = sp.apply(rn, x);
+            if (!rc) rc = sp.saxpy(rn, one, rn, b);  // rn = b - A x
+            if (!rc) rc = sp.copy(p, rn);
+            if (!rc) rc = sp.dot(rn, rn, &omega);
+            if (rc) return rc;
+        }
+        rc = sp.apply(v, p);
+        if (!rc) rc = sp.dot(p, v, &rho);
+        if (rc) return rc;
+        alpha = cdiv(omega, rho);
+        rc    = sp.saxpy(x, Cx{-alpha.re, -alpha.im}, p, x);  // x += alpha p
+        if (!rc) rc = sp.saxpy(rn, alpha, v, rn);           // rn -= alpha v
+        if (!rc) rc = sp.dot(rn, rn, &omega_next);
+        if (rc) return rc;
+        beta  = cdiv(omega_next, omega);
+        omega = omega_next;
+        if (iter % P->resid_check_every == 0) {
+            resid = omega.re;
+            if (resid != resid) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            if (resid < thr && iter >= P->min_iter) {
+                if (P->rel_tol > 0) {
+                    double r2t = 0;
+                    rc         = true_r2(&r2t);
+                    if (rc) return rc;
+                    if (!(r2t <= P->rel_tol * P->rel_tol * b2 || (P->prec > 0 && r2t < P->prec))) {
+                        force_refresh = true;  // the iterated residual drifted: restart from the true residual
+                        continue;
+                    }
+                }
+                status = iter;
+                break;
+            }
+        }
+        rc = sp.saxpy(p, Cx{-beta.re, -beta.im}, p, rn);  // p = rn + beta p
+        if (rc) return rc;
+    }
+    double r2t = 0;
+    rc         = true_r2(&r2t);
+    if (rc) return rc;
+    finish_report(rep, status, iter, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sp.sweeps);
+    if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
+    if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "NAN occured in the CG residual");
     return status;
 }
 
@@ -990,6 +1176,76 @@ C2Q_EXPORT int c2q_cg_multi(c2q_spinor_eo* const* x, int op, const c2q_gauge* g,
 }
 
 // Eo branch of invert_M_nf2_upperflavour (physics/algorithms/inversion.cpp:129-236).
+// ---- full-lattice solves (useEO=false)
+static int full_solve(bool cg, c2q_spinor_eo* x_even, c2q_spinor_eo* x_odd, int op, const c2q_gauge* g,
+                      const c2q_spinor_eo* b_even, const c2q_spinor_eo* b_odd, double kappa, double mubar, int action,
+                      const c2q_solver_params* p, c2q_solve_report* report)
+{
+    if (!x_even || !x_odd || !b_even || !b_odd) return C2Q_BAD_ARG;
+    c2q_ctx* ctx = x_even->ctx;
+    int rc       = 0;
+    if (!validate(ctx, x_even, g, b_even, p, &rc) || !validate(ctx, x_odd, g, b_odd, p, &rc)) return rc;
+    if (x_even == x_odd || b_even == b_odd || x_even == b_even || x_odd == b_odd || x_even == b_odd ||
+        x_odd == b_even)
+        return fail(ctx, C2Q_BAD_ARG, "solution and source halves must be four different fields");
+    if (op < C2Q_FULL_M_TM_PLUS || op > C2Q_FULL_QPLUSQMINUS)
+        return fail(ctx, C2Q_BAD_ARG, "unknown full-lattice fermion matrix");
+    if (p->precision != 64) return fail(ctx, C2Q_BAD_ARG, "the full-lattice solvers run in FP64");
+    FullSpace sp{ctx, &x_even->lat, op, g, kappa, mubar, action};
+    sp.half.ctx = ctx;
+    const FullSpace::V x{x_even, x_odd}, b{const_cast<c2q_spinor_eo*>(b_even), const_cast<c2q_spinor_eo*>(b_odd)};
+    return cg ? cg_generic(sp, x, b, p, report) : bicgstab_generic(sp, x, b, p, report);
+}
+
+C2Q_EXPORT int c2q_cg_full(c2q_spinor_eo* x_even, c2q_spinor_eo* x_odd, int op, const c2q_gauge* g,
+                           const c2q_spinor_eo* b_even, const c2q_spinor_eo* b_odd, double kappa, double mubar,
+                           int action, const c2q_solver_params* p, c2q_solve_report* report)
+{
+    return full_solve(true, x_even, x_odd, op, g, b_even, b_odd, kappa, mubar, action, p, report);
+}
+
+C2Q_EXPORT int c2q_bicgstab_full(c2q_spinor_eo* x_even, c2q_spinor_eo* x_odd, int op, const c2q_gauge* g,
+                                 const c2q_spinor_eo* b_even, const c2q_spinor_eo* b_odd, double kappa, double mubar,
+                                 int action, const c2q_solver_params* p, c2q_solve_report* report)
+{
+    return full_solve(false, x_even, x_odd, op, g, b_even, b_odd, kappa, mubar, action, p, report);
+}
+
+// invert_M_nf2_upperflavour, non-eo branch (inversion.cpp:98-122): from a cold
+// start, CG on QplusQminus with the source gamma5 b followed by Qminus, or
+// BiCGStab on M; result = M^-1 source (host full fields).
+C2Q_EXPORT int c2q_perform_inversion_full(c2q_ctx* ctx, double* result, const c2q_gauge* g, const double* source,
+                                          double kappa, double mubar, int action, const c2q_solver_params* p,
+                                          c2q_solve_report* report)
+{
+    if (!ctx || !result || !g || !source || !p) return C2Q_BAD_ARG;
+    Fields F;
+    int rc = make_fields(ctx, g->lat, 64, 6, F, 0);
+    if (rc) return rc;
+    c2q_spinor_eo *xe = &F.f[0], *xo = &F.f[1], *be = &F.f[2], *bo = &F.f[3], *te = &F.f[4], *to = &F.f[5];
+    rc = c2q_convert_to_eoprec(be, bo, source);
+    if (!rc) rc = c2q_spinor_eo_cold(xe);
+    if (!rc) rc = c2q_spinor_eo_cold(xo);
+    if (rc) return rc;
+    int conv = 0;
+    if (p->solver == C2Q_SOLVER_CG) {
+        // tmp = gamma5 b; QplusQminus y = tmp; x = Qminus y
+        rc = c2q_gamma5_eo(be);
+        if (!rc) rc = c2q_gamma5_eo(bo);
+        if (rc) return rc;
+        conv = c2q_cg_full(xe, xo, C2Q_FULL_QPLUSQMINUS, g, be, bo, kappa, mubar, action, p, report);
+        if (conv < 0) return conv;
+        rc = copy_field(ctx, te, xe);
+        if (!rc) rc = copy_field(ctx, to, xo);
+        if (!rc) rc = c2q_apply_full(C2Q_FULL_QMINUS, xe, xo, g, te, to, kappa, mubar, action);
+    } else {
+        conv = c2q_bicgstab_full(xe, xo, C2Q_FULL_M_TM_PLUS, g, be, bo, kappa, mubar, action, p, report);
+        if (conv < 0) return conv;
+    }
+    if (!rc) rc = c2q_convert_from_eoprec(result, xe, xo);
+    return rc ? rc : conv;
+}
+
 C2Q_EXPORT int c2q_perform_inversion_eo(c2q_ctx* ctx, double* result, const c2q_gauge* g, const double* source,
                                         double kappa, double mubar, int action, const c2q_solver_params* p,
                                         c2q_solve_report* report)

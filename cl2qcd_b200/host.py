@@ -408,11 +408,15 @@ class SolverParameters:
                                int(self.use_rec12), int(self.use_graph), int(self.temporal_gauge))
 
 
-def _solve(fn, x, A, gf, b, params, add, report):
+def _solve(fn, x, A, gf, b, params, add, report, fn_full=None):
     lib = x.system.lib
     p = params.c()
     rep = L.CSolveReport()
-    rc = fn(x.h, A.OP, gf.h, b.h, add.kappa, add.mubar, A.action, C.byref(p), C.byref(rep))
+    if isinstance(x, Spinorfield):  # full fields (useEO=false): a full-lattice matrix
+        rc = fn_full(x.even.h, x.odd.h, A.OP, gf.h, b.even.h, b.odd.h, add.kappa, add.mubar, A.action,
+                     C.byref(p), C.byref(rep))
+    else:
+        rc = fn(x.h, A.OP, gf.h, b.h, add.kappa, add.mubar, A.action, C.byref(p), C.byref(rep))
     if report is not None:
         report.update(rep.as_dict())
     if rc == L.SOLVER_STUCK:
@@ -423,7 +427,8 @@ def _solve(fn, x, A, gf, b, params, add, report):
 
 
 def cg(x, A, gf, b, params: SolverParameters, add: AdditionalParameters, report: dict | None = None) -> int:
-    return _solve(x.system.lib.c2q_cg, x, A, gf, b, params, add, report)
+    """solvers::cg on eo fields (A an eo matrix) or on full fields (A a full-lattice matrix)."""
+    return _solve(x.system.lib.c2q_cg, x, A, gf, b, params, add, report, x.system.lib.c2q_cg_full)
 
 
 def cg_multi(xs, A, gf, bs, params: SolverParameters, add: AdditionalParameters,
@@ -464,20 +469,25 @@ def point_source(n_sites: int, k: int) -> np.ndarray:
 
 
 def bicgstab(x, A, gf, b, params: SolverParameters, add: AdditionalParameters, report: dict | None = None) -> int:
-    return _solve(x.system.lib.c2q_bicgstab, x, A, gf, b, params, add, report)
+    """solvers::bicgstab on eo fields (A an eo matrix) or on full fields (A a full-lattice matrix)."""
+    return _solve(x.system.lib.c2q_bicgstab, x, A, gf, b, params, add, report, x.system.lib.c2q_bicgstab_full)
 
 
 def perform_inversion(system: System, gf: Gaugefield, source: np.ndarray, params: SolverParameters,
-                      add: AdditionalParameters, action: str = "twistedmass", report: dict | None = None):
-    """One source of perform_inversion (eo); returns the full result field (reference sign convention)."""
+                      add: AdditionalParameters, action: str = "twistedmass", report: dict | None = None,
+                      use_eo: bool = True):
+    """One source of perform_inversion; returns the full result field.  use_eo
+    (the reference's useEO): the eo Schur solve with the reference's sign
+    convention (inversion.cpp:123-236), else the full-lattice solve
+    (inversion.cpp:98-122, result = M^-1 source)."""
     lib = system.lib
     src = np.ascontiguousarray(source, dtype=np.float64).reshape(-1)
     out = np.zeros_like(src)
     p = params.c()
     rep = L.CSolveReport()
     act = L.WILSON if action.lower() == "wilson" else L.TWISTEDMASS
-    rc = lib.c2q_perform_inversion_eo(system.h, out, gf.h, src, add.kappa, add.mubar, act, C.byref(p),
-                                      C.byref(rep))
+    fn = lib.c2q_perform_inversion_eo if use_eo else lib.c2q_perform_inversion_full
+    rc = fn(system.h, out, gf.h, src, add.kappa, add.mubar, act, C.byref(p), C.byref(rep))
     if report is not None:
         report.update(rep.as_dict())
     if rc == L.SOLVER_STUCK:
@@ -499,12 +509,13 @@ def point_source_full(lattice: Lattice, k: int, x: int = 0, y: int = 0, z: int =
 
 def inverter_ps_correlator(system: System, gf: Gaugefield, params: SolverParameters, add: AdditionalParameters,
                            n_sources: int = 12, position=(0, 0, 0, 0), action: str = "twistedmass",
-                           reports: list | None = None, direction: int = 3) -> np.ndarray:
+                           reports: list | None = None, direction: int = 3, use_eo: bool = True) -> np.ndarray:
     """The inverter's point-source measurement (physics/observables/wilsonTwoFlavourCorrelators.cpp:
     measureTwoFlavourDoubletCorrelatorsOnGaugefieldAndWriteToFile with the default 12 point
-    sources): perform_inversion (eo) of each spin-colour point source, results kept on the
-    device, and the pseudoscalar correlator contracted on the GPU along z (direction 3,
-    the reference's default correlatorDirection) or t (direction 0)."""
+    sources): perform_inversion of each spin-colour point source (eo, results kept on the
+    device; or, use_eo False, the full-lattice solve), and the pseudoscalar correlator
+    contracted on the GPU along z (direction 3, the reference's default correlatorDirection)
+    or t (direction 0)."""
     lib = system.lib
     L_ = gf.lattice
     act = L.WILSON if action.lower() == "wilson" else L.TWISTEDMASS
@@ -514,8 +525,15 @@ def inverter_ps_correlator(system: System, gf: Gaugefield, params: SolverParamet
     for k in range(n_sources):
         src = point_source_full(L_, k % 12, *position).reshape(-1)
         rep = L.CSolveReport()
-        rc = lib.c2q_perform_inversion_eo_fields(system.h, evens[k].h, odds[k].h, gf.h, src, add.kappa, add.mubar,
-                                                 act, C.byref(p), C.byref(rep))
+        if use_eo:
+            rc = lib.c2q_perform_inversion_eo_fields(system.h, evens[k].h, odds[k].h, gf.h, src, add.kappa,
+                                                     add.mubar, act, C.byref(p), C.byref(rep))
+        else:
+            res = np.zeros_like(src)
+            rc = lib.c2q_perform_inversion_full(system.h, res, gf.h, src, add.kappa, add.mubar, act, C.byref(p),
+                                                C.byref(rep))
+            if rc >= 0:
+                _check(lib.c2q_convert_to_eoprec(evens[k].h, odds[k].h, res), system.h, lib)
         if reports is not None:
             reports.append(rep.as_dict())
         if rc == L.SOLVER_STUCK:

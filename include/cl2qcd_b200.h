@@ -319,6 +319,24 @@ C2Q_EXPORT int c2q_perform_inversion_eo_fields(c2q_ctx* ctx, c2q_spinor_eo* out_
 C2Q_EXPORT int c2q_correlator_ps(const c2q_spinor_eo* const* even, const c2q_spinor_eo* const* odd, int n,
                                  double kappa, int direction, double* out);
 
+/* Full-lattice (useEO=false) solves: solvers::cg / bicgstab on
+ * physics::lattices::Spinorfield (physics/algorithms/inversion.cpp:98-122), x
+ * and b held as their two parities (c2q_convert_to_eoprec), op a C2Q_FULL_*
+ * matrix; FP64, the reference's semantics, x holds the start vector. */
+C2Q_EXPORT int c2q_cg_full(c2q_spinor_eo* x_even, c2q_spinor_eo* x_odd, int op, const c2q_gauge* g,
+                           const c2q_spinor_eo* b_even, const c2q_spinor_eo* b_odd, double kappa, double mubar,
+                           int action, const c2q_solver_params* p, c2q_solve_report* report);
+C2Q_EXPORT int c2q_bicgstab_full(c2q_spinor_eo* x_even, c2q_spinor_eo* x_odd, int op, const c2q_gauge* g,
+                                 const c2q_spinor_eo* b_even, const c2q_spinor_eo* b_odd, double kappa, double mubar,
+                                 int action, const c2q_solver_params* p, c2q_solve_report* report);
+/* perform_inversion, non-eo branch of invert_M_nf2_upperflavour (inversion.cpp:98-122):
+ * cold start; solver CG: QplusQminus y = gamma5 source, result = Qminus y;
+ * otherwise BiCGStab (p->solver fast / save) on M.  Host full fields spinor[V];
+ * result = M^{-1} source. */
+C2Q_EXPORT int c2q_perform_inversion_full(c2q_ctx* ctx, double* result, const c2q_gauge* g, const double* source,
+                                          double kappa, double mubar, int action, const c2q_solver_params* p,
+                                          c2q_solve_report* report);
+
 /* ---------------- HMC callers of the eo solvers ----------------
  * Gauge momenta (physics::lattices::Gaugemomenta, physics/lattices/gaugemomenta.hpp):
  * 8 reals (the su(3) algebra element ae, common_header_files/types.hpp:178-188)

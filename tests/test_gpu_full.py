@@ -90,3 +90,52 @@ def test_inversion_solves_the_full_system(system, port):
     P, R = c2q.host.Spinorfield(system, L, phi), c2q.host.Spinorfield(system, L)
     c2q.host.M_tm_plus()(R, gf, P, add)
     assert np.linalg.norm(R.dump() + b) / np.linalg.norm(b) <= 1e-10
+
+
+@pytest.mark.parametrize("solver", ["bicgstab", "cg", "bicgstab_save"])
+def test_full_lattice_inversion(system, port, solver):
+    """useEO=false (inversion.cpp:98-122): the full-lattice solve returns M^{-1} b,
+    and agrees with the eo solve (whose convention is -M^{-1} b)."""
+    import cl2qcd_b200 as c2q
+    ns, nt = 8, 8
+    port.set_lattice(ns, nt, 1.0, 0.0)
+    L = c2q.Lattice(ns, nt, 1.0, 0.0)
+    g = c2q.host.generate_gaugefield(L, 0.3, 5)
+    gf = c2q.Gaugefield(system, L, g)
+    b = port.pseudo_randomize(L.vol, 9)
+    add = c2q.AdditionalParameters(0.15, 2 * 0.15 * 0.01)
+    params = c2q.SolverParameters(solver=solver, prec=1e-24, cgmax=4000)
+    rep = {}
+    phi, _ = c2q.host.perform_inversion(system, gf, b, params, add, report=rep, use_eo=False)
+    r = port.m_tm_plus(np.ascontiguousarray(phi.reshape(-1, 24)), g, 0.15, 2 * 0.15 * 0.01)
+    assert np.linalg.norm(r - b) / np.linalg.norm(b) <= 1e-10, rep
+    phi_eo, _ = c2q.host.perform_inversion(system, gf, b, params, add)
+    assert np.linalg.norm(phi + phi_eo) / np.linalg.norm(phi) <= 1e-9
+
+
+@pytest.mark.parametrize("solver", ["cg", "bicgstab"])
+def test_full_lattice_solvers(system, port, solver):
+    """solvers::cg on QplusQminus and bicgstab on M_tm_plus with full fields."""
+    import cl2qcd_b200 as c2q
+    ns, nt = 4, 8
+    port.set_lattice(ns, nt, 1.0, 0.3)
+    L = c2q.Lattice(ns, nt, 1.0, 0.3)
+    g = c2q.host.generate_gaugefield(L, 0.3, 7)
+    gf = c2q.Gaugefield(system, L, g)
+    kappa, mubar = 0.15, 2 * 0.15 * 0.02
+    add = c2q.AdditionalParameters(kappa, mubar)
+    bh = port.pseudo_randomize(L.vol, 3)
+    b = c2q.host.Spinorfield(system, L, bh)
+    x = c2q.host.Spinorfield(system, L)
+    params = c2q.SolverParameters(solver=solver, prec=0.0, rel_tol=1e-11, cgmax=4000)
+    rep = {}
+    if solver == "cg":
+        it = c2q.host.cg(x, c2q.host.QplusQminus(), gf, b, params, add, rep)
+        g5 = np.where(np.arange(24) < 12, 1.0, -1.0)  # spins 2, 3 flip sign
+        xm = port.m_tm_minus(x.dump(), g, kappa, mubar) * g5
+        ax = port.m_tm_plus(np.ascontiguousarray(xm), g, kappa, mubar) * g5  # Q+ Q- x = g5 M+ g5 M- x
+    else:
+        it = c2q.host.bicgstab(x, c2q.host.M_tm_plus(), gf, b, params, add, rep)
+        ax = port.m_tm_plus(x.dump(), g, kappa, mubar)
+    assert it > 0 and rep["true_resid_rel"] <= 1e-11
+    assert np.linalg.norm(ax - bh) / np.linalg.norm(bh) <= 1e-10

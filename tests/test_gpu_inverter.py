@@ -7,7 +7,9 @@ twisted mass kappa 0.15, mu 4, periodic boundaries, the 12 default point sources
 at the origin, eo perform_inversion of each (result kept on the device), the
 pseudoscalar correlator along z (the reference's default direction) contracted on
 the GPU.  The reference's test compares at 0.1 %; the solvers it runs
-(bicgstab, cg, bicgstab_save) are all checked here, at 1e-9.
+(bicgstab, cg, bicgstab_save), each with useEO true and false (the
+full-lattice solve of inversion.cpp:98-122) as its CMakeLists registers them,
+are all checked here, at 1e-9.
 """
 import json
 import os
@@ -20,9 +22,10 @@ pytestmark = pytest.mark.gpu
 KATS = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_kats.json")))
 
 
+@pytest.mark.parametrize("use_eo", [True, False])
 @pytest.mark.parametrize("solver", ["bicgstab", "cg", "bicgstab_save"])
 @pytest.mark.parametrize("name", ["inverter_test_ref", "inverter_test_ref2"])
-def test_ps_correlator_matches_inverter_reference(system, solver, name):
+def test_ps_correlator_matches_inverter_reference(system, solver, name, use_eo):
     import cl2qcd_b200 as c2q
     ref = KATS["inverter"][name]
     ns, nt = int(ref["input"]["nSpace"]), int(ref["input"]["nTime"])
@@ -37,7 +40,7 @@ def test_ps_correlator_matches_inverter_reference(system, solver, name):
     params = c2q.SolverParameters(solver=solver, prec=1e-23, cgmax=1000)
     reps = []
     C = c2q.host.inverter_ps_correlator(system, gf, params, c2q.AdditionalParameters.from_mu(kappa, mu),
-                                        reports=reps)
+                                        reports=reps, use_eo=use_eo)
     assert len(reps) == 12
     np.testing.assert_allclose(C, ref["ps_correlator"], rtol=ref["tolerance_percent"] / 100)
     np.testing.assert_allclose(C, ref["ps_correlator"], rtol=1e-9)
