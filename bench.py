@@ -288,6 +288,8 @@ def serving_run(c2q, rates, n_requests, slots=4, seed=4242, log=None):
     """Poisson-arriving inversion requests: volume uniform over SERVE_VOLUMES
     (one resident gauge field per volume, eps ~ U[0.2, 0.35]), kappa ~ U[0.14, 0.16],
     mu ~ U[0.002, 0.02], 1-12 Z2 sources, mixed-precision (FP16 inner) to 1e-10.
+    The request list and the unit-rate arrival gaps are drawn once, so every
+    rate serves the same requests and only the arrival spacing changes.
     For each arrival rate: latency = completion - submission per request,
     p50 / p99 (nearest rank), and solves/s = sources solved / wall time."""
     rng = np.random.default_rng(seed)
@@ -306,11 +308,12 @@ def serving_run(c2q, rates, n_requests, slots=4, seed=4242, log=None):
            "sources": "Z2, 1-12 per request", "gauge_setup_s": round(t_setup, 1),
            "budget_bytes": server.stats()["budget_bytes"], "gauge_bytes": server.stats()["gauge_bytes"],
            "rates": []}
+    reqs = [(int(rng.integers(0, len(SERVE_VOLUMES))), float(rng.uniform(0.14, 0.16)),
+             float(rng.uniform(0.002, 0.02)), int(rng.integers(1, 13)), int(rng.integers(1, 1 << 40)))
+            for _ in range(n_requests)]
+    unit_gaps = rng.exponential(1.0, n_requests)
     for rate in rates:
-        gaps = rng.exponential(1.0 / rate, n_requests)
-        reqs = [(int(rng.integers(0, len(SERVE_VOLUMES))), float(rng.uniform(0.14, 0.16)),
-                 float(rng.uniform(0.002, 0.02)), int(rng.integers(1, 13)), int(rng.integers(1, 1 << 40)))
-                for _ in range(n_requests)]
+        gaps = unit_gaps / rate
         t0 = time.time()
         tickets, next_t = [], 0.0
         for gap, (v, kappa, mu, n, sd) in zip(gaps, reqs):
