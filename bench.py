@@ -184,6 +184,73 @@ def cpu_reference_sample(g, b, fp64_iters, budget_s=15.0):
             "seconds_per_iteration": per_iter}
 
 
+def cpu_reference_extras(g, b, budget_s=10.0):
+    """Beside the solve-rate sample: the reference's dslash_eo on the host cores in
+    GB/s by the algorithmic byte model (1536 B/site, FP64 18-real), and config 1
+    (8^4, eps 0.3, kappa 0.15, mu 0.01, one Z2 source) solved to a true residual
+    1e-10 by the reference CG on its own kernels."""
+    import oracle as O
+    import cl2qcd_b200 as c2q
+    kind = "reference" if O.available("reference") else "port"
+    o = O.Oracle(kind)
+    o.set_lattice(NS, NT, 1.0, 0.0)
+    o.dslash_eo(b, g, O.ODD, KAPPA)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while n < 3 and (n == 0 or time.perf_counter() - t0 < budget_s):
+        o.dslash_eo(b, g, O.ODD, KAPPA)
+        n += 1
+    t = time.perf_counter() - t0
+    gbs = DSLASH_BYTES[(64, 0)] * b.shape[0] * n / t / 1e9
+    c1 = config1_inputs(c2q)
+    o.set_lattice(8, 8, 1.0, 0.0)
+    b2 = float((c1["b"] ** 2).sum())
+    P = O.SolverParams(prec=REL_TOL ** 2 * b2, cgmax=10000, solver=1)
+    x = np.zeros_like(c1["b"])
+    o.cg(x, O.OP_QPQM_EO, c1["b"], c1["g"], 0.15, 2 * 0.15 * 0.01, params=P)  # warm-up
+    m, t0 = 0, time.perf_counter()
+    while m < 20 and (m == 0 or time.perf_counter() - t0 < budget_s):
+        x[:] = 0
+        o.cg(x, O.OP_QPQM_EO, c1["b"], c1["g"], 0.15, 2 * 0.15 * 0.01, params=P)
+        m += 1
+    t1 = time.perf_counter() - t0
+    o.set_lattice(NS, NT, 1.0, 0.0)
+    return {"dslash_gbs": round(gbs, 2), "dslash_sample": f"{n} FP64 18-real dslash_eo sweeps of 32^3x64",
+            "config1_solves_per_s": round(m / t1, 2), "config1_sample": f"{m} solves of 8^4 to 1e-10"}
+
+
+def config1_inputs(c2q):
+    """config 1: 8^4, eps 0.3 links, one Z2 source (kappa 0.15, mu 0.01)."""
+    lat = c2q.Lattice(8, 8, 1.0, 0.0)
+    return {"lat": lat, "g": c2q.host.generate_gaugefield(lat, 0.3, 1),
+            "b": c2q.host.generate_source(lat.seo, "z2", 2)}
+
+
+def config1_gpu(c2q, system, e0, e1, n=20):
+    """config 1 on the GPU: FP64 eo CG (the reference's algorithm) to a true residual 1e-10."""
+    import torch
+    c1 = config1_inputs(c2q)
+    gf = c2q.Gaugefield(system, c1["lat"], c1["g"])
+    B = c2q.Spinorfield_eo(system, c1["lat"], c1["b"])
+    X = c2q.Spinorfield_eo(system, c1["lat"])
+    add = c2q.AdditionalParameters(0.15, 2 * 0.15 * 0.01)
+    A = c2q.host.QplusQminus_eo()
+    P = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=10000, precision=64)
+    rep = {}
+    for _ in range(3):
+        X.zero()
+        c2q.host.cg(X, A, gf, B, P, add, rep)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(n):
+        X.zero()
+        c2q.host.cg(X, A, gf, B, P, add)
+    e1.record()
+    torch.cuda.synchronize()
+    return {"workload": "8^4, eps 0.3, kappa 0.15, mu 0.01, one Z2 source, FP64 eo CG to 1e-10",
+            "gpu_fp64_solves_per_s": round(n / (e0.elapsed_time(e1) / 1e3), 1),
+            "iterations": rep["iterations"], "true_resid_rel": rep["true_resid_rel"]}
+
+
 # algorithmic bytes per site of one plain dslash_eo sweep: 8 links + input + output
 DSLASH_BYTES = {(64, 0): 8 * 144 + 2 * 192, (64, 1): 8 * 96 + 2 * 192, (32, 0): 8 * 72 + 2 * 96,
                 (32, 1): 8 * 48 + 2 * 96, (16, 1): 8 * 24 + 2 * 52}
@@ -618,6 +685,7 @@ def main():
         return out
 
     mrhs = mrhs_section()
+    config1 = config1_gpu(c2q, system, e0, e1)
     # serving stream at one arrival rate (the full sweep: --serve)
     serving = serving_run(c2q, [1.0], args.serve_requests) if rank == 0 and ws == 1 else None
 
@@ -626,6 +694,7 @@ def main():
         try:
             cpu_baseline = cpu_reference_sample(g, b, ref_iters)
             cpu_baseline.pop("seconds_per_iteration", None)
+            cpu_baseline.update(cpu_reference_extras(g, b))
         except Exception as e:  # the baseline is reported, never required
             cpu_baseline = {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "reference",
                             "sample": f"unavailable: {e}"}
@@ -665,6 +734,7 @@ def main():
             "speedup_mixed_vs_fp64": value / ws * fp64_s,
             "dslash_gbs": dg,
             "multi_rhs": mrhs,
+            "config1": config1,
             "serving": serving,
             "autotune": system.tune_report().strip().splitlines(),
         }
