@@ -240,22 +240,61 @@ int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2
         // residual is confirmed by an FP64 true residual, else CG restarts from it.
         ResidRing ring(ctx);
         int skip_upto = -1;
+        // With use_graph the iteration body between refreshes (p = rn + beta p,
+        // v = A p with (p, v) -> alpha, the x / rn update) replays as one captured
+        // CUDA graph: small lattices are bound by launch latency.  It is captured
+        // after the first (eager) iteration has sized every launch.
+        const bool graphs = P->use_graph && !ctx->profiling;
+        struct Exec {
+            cudaGraphExec_t e = nullptr;
+            ~Exec()
+            {
+                if (e) cudaGraphExecDestroy(e);
+            }
+        } gexec;
+        long long gkernels = 0;
+        int gsweeps        = 0;
+        auto apply_update = [&](int* sw) -> int {
+            DotSpec d;
+            d.mode = DOT_Y;
+            d.y    = p;
+            d.fin  = FIN_CG_ALPHA;
+            int e  = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, sw);
+            return e ? e : launch_cg_update(ctx, x, rn, p, v);
+        };
         for (iter = 0; iter < P->cgmax || iter < P->min_iter; iter++) {
             if (iter % P->iter_refresh == 0 || force_refresh) {
                 force_refresh = false;
                 rc = apply_operator(ctx, op, rn, g, gk, x, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
                 if (!rc) rc = saxpy_norm(ctx, rn, Cx{1, 0}, rn, b, FIN_CG_OMEGA, nullptr);
                 if (!rc) rc = copy_field(ctx, p, rn);
+                if (!rc) rc = apply_update(&sweeps);
+            } else if (graphs) {
+                if (!gexec.e) {
+                    cudaGraph_t gr     = nullptr;
+                    const long long l0 = ctx->launches;
+                    C2Q_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+                    int eb = launch_cg_p(ctx, p, rn);
+                    if (!eb) eb = apply_update(&gsweeps);
+                    const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &gr);
+                    if (eb) {
+                        if (gr) cudaGraphDestroy(gr);
+                        return eb;
+                    }
+                    C2Q_CUDA(ctx, ec);
+                    const cudaError_t ei = cudaGraphInstantiate(&gexec.e, gr, 0);
+                    cudaGraphDestroy(gr);
+                    C2Q_CUDA(ctx, ei);
+                    gkernels      = ctx->launches - l0;
+                    ctx->launches = l0;
+                }
+                C2Q_CUDA(ctx, cudaGraphLaunch(gexec.e, ctx->stream));
+                ctx->launches += gkernels;
+                sweeps += gsweeps;
             } else {
                 rc = launch_cg_p(ctx, p, rn);  // p = rn + beta p
+                if (!rc) rc = apply_update(&sweeps);
             }
-            if (rc) return rc;
-            DotSpec d;
-            d.mode = DOT_Y;
-            d.y    = p;
-            d.fin  = FIN_CG_ALPHA;
-            rc     = apply_operator(ctx, op, v, g, gk, p, kappa, mubar, action, t1, t2, d, &sweeps);
-            if (!rc) rc = launch_cg_update(ctx, x, rn, p, v);
             if (!rc) rc = ring.push(iter);
             if (rc) return rc;
             if (iter == 0) continue;

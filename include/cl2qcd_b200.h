@@ -118,7 +118,7 @@ typedef struct {
     int precision;            /* C2Q_PREC_*: inner arithmetic */
     double reliable_delta;    /* mixed precision: reliable update when |r_inner| < delta * max|r| since the last one (default 0.003) */
     int use_rec12;            /* inner operator uses 12-real links */
-    int use_graph;            /* capture the iterations between residual checks in a CUDA graph */
+    int use_graph;            /* CG: replay the iterations between residual refreshes as a captured CUDA graph */
     int use_temporal_gauge;   /* mixed precision on QplusQminus_eo: inner iterations on the field in the
                                  temporal gauge (T links the identity but on the last slice), where the
                                  T weights are pure phases and the spatial ones real (default 1) */

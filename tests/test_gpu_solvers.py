@@ -89,6 +89,28 @@ def test_cg_true_residual_1e10(port, system, O, precision, rec12):
     assert np.linalg.norm(r - b) / np.linalg.norm(b) <= 1.5e-10
 
 
+@pytest.mark.parametrize("iter_refresh", [100, 7])
+def test_fp64_cg_graph_replay_matches_eager(port, system, O, iter_refresh):
+    """FP64 CG with use_graph: the iterations between refreshes replay as a
+    captured graph of the same kernels, so the iterates are bitwise those of the
+    eager loop (also across refreshes, iter_refresh 7)."""
+    import cl2qcd_b200 as c2q
+    L, g, gf, b = _prob(port, c2q, system, 8, 8, 0.3, 1)
+    add = c2q.AdditionalParameters(0.15, 2 * 0.15 * 0.01)
+    B = c2q.Spinorfield_eo(system, L, b)
+    out = {}
+    for graph in (False, True):
+        X = c2q.Spinorfield_eo(system, L)
+        rep = {}
+        c2q.host.cg(X, c2q.host.QplusQminus_eo(), gf, B,
+                    c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=1e-10, cgmax=20000, precision=64,
+                                         iter_refresh=iter_refresh, use_graph=graph), add, rep)
+        assert rep["true_resid_rel"] <= 1e-10, rep
+        out[graph] = (X.dump(), rep["iterations"], rep["dslash_applications"])
+    assert out[True][1] == out[False][1] and out[True][2] == out[False][2]
+    assert np.array_equal(out[True][0], out[False][0])
+
+
 def test_solver_errors(port, system, O):
     """Host-side failure injection: NaN in the source -> SolverStuck; cgmax too small -> SolverDidNotSolve."""
     import cl2qcd_b200 as c2q
