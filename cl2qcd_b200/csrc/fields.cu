@@ -996,6 +996,25 @@ C2Q_EXPORT int c2q_spinor_eo_download(const c2q_spinor_eo* f, double* aos)
     return C2Q_OK;
 }
 
+// The same transfers, enqueued on the context's stream without waiting (FP64
+// fields): a caller driving several contexts overlaps one context's copies with
+// another's solve.
+C2Q_EXPORT int c2q_spinor_eo_upload_async(c2q_spinor_eo* f, const double* aos)
+{
+    if (!f || !aos) return C2Q_BAD_ARG;
+    if (f->prec != 64) return fail(f->ctx, C2Q_BAD_ARG, "asynchronous transfers take FP64 fields");
+    return aos_transfer(f, nullptr, aos, 0, 0, nullptr);
+}
+
+C2Q_EXPORT int c2q_spinor_eo_download_async(const c2q_spinor_eo* f, double* aos)
+{
+    if (!f || !aos) return C2Q_BAD_ARG;
+    c2q_spinor_eo* ff = const_cast<c2q_spinor_eo*>(f);
+    if (f->prec != 64) return fail(f->ctx, C2Q_BAD_ARG, "asynchronous transfers take FP64 fields");
+    const int rc = ensure_staging(ff->ctx, (size_t)f->geom.seo * 24 * sizeof(double));
+    return rc ? rc : aos_transfer(ff, aos, nullptr, 0, 0, nullptr);
+}
+
 C2Q_EXPORT int c2q_spinor_eo_precision(const c2q_spinor_eo* f) { return f ? f->prec : C2Q_BAD_ARG; }
 
 C2Q_EXPORT int c2q_spinor_eo_convert(c2q_spinor_eo* out, const c2q_spinor_eo* in)

@@ -177,6 +177,13 @@ C2Q_EXPORT int c2q_spinor_eo_destroy(c2q_spinor_eo* f);
 /* Spinor::load / dump (hardware/buffers/spinor.cpp:83-106): spinor[Seo] in eo index order. */
 C2Q_EXPORT int c2q_spinor_eo_upload(c2q_spinor_eo* f, const double* aos);
 C2Q_EXPORT int c2q_spinor_eo_download(const c2q_spinor_eo* f, double* aos);
+/* (no counterpart in the reference: its Spinor::load / dump wait) The same
+ * transfers enqueued on the context's stream without waiting, FP64 fields only.
+ * The host array must stay valid, and a download's must not be read, until the
+ * stream has passed the copy (c2q_ctx_synchronize); with pinned host memory the
+ * copy overlaps work of other contexts on the GPU. */
+C2Q_EXPORT int c2q_spinor_eo_upload_async(c2q_spinor_eo* f, const double* aos);
+C2Q_EXPORT int c2q_spinor_eo_download_async(const c2q_spinor_eo* f, double* aos);
 /* Spinorfield_eo::zero / cold (physics/lattices/spinorfield_eo.cpp:147-165) */
 C2Q_EXPORT int c2q_spinor_eo_zero(c2q_spinor_eo* f);
 C2Q_EXPORT int c2q_spinor_eo_cold(c2q_spinor_eo* f);

@@ -90,3 +90,22 @@ def test_bad_arguments_raise(env, system):
         c2q.host.saxpy(other, 1.0, X, Y)
     with pytest.raises(c2q.host.InvalidParameters):
         c2q.Spinorfield_eo(system, c2q.Lattice(5, 4))
+
+
+def test_async_transfers_round_trip(system, port):
+    """c2q_spinor_eo_upload_async / download_async: enqueued without waiting, the
+    data arrive after the context synchronises; FP32 fields are refused."""
+    import cl2qcd_b200 as c2q
+    lib = system.lib
+    L = c2q.Lattice(4, 8)
+    port.set_lattice(4, 8)
+    a = np.ascontiguousarray(port.pseudo_randomize(L.seo, 5))
+    f = c2q.Spinorfield_eo(system, L)
+    assert lib.c2q_spinor_eo_upload_async(f.h, a) == 0
+    out = np.zeros_like(a)
+    assert lib.c2q_spinor_eo_download_async(f.h, out) == 0
+    system.synchronize()
+    assert np.array_equal(out, a)
+    g = c2q.Spinorfield_eo(system, L, a, precision=32)
+    assert lib.c2q_spinor_eo_upload_async(g.h, a) != 0
+    assert lib.c2q_spinor_eo_download_async(g.h, out) != 0
