@@ -99,8 +99,8 @@ SIGNATURES = {
     "c2q_spinor_eo_destroy": (C.c_int, [_P]),
     "c2q_spinor_eo_upload": (C.c_int, [_P, _D]),
     "c2q_spinor_eo_download": (C.c_int, [_P, _D]),
-    "c2q_spinor_eo_upload_async": (C.c_int, [_P, _D]),
-    "c2q_spinor_eo_download_async": (C.c_int, [_P, _D]),
+    "c2q_spinor_eo_upload_async": (C.c_int, [_P, _D, _P]),
+    "c2q_spinor_eo_download_async": (C.c_int, [_P, _D, _P]),
     "c2q_spinor_eo_zero": (C.c_int, [_P]),
     "c2q_spinor_eo_cold": (C.c_int, [_P]),
     "c2q_convert_to_eoprec": (C.c_int, [_P, _P, _D]),

@@ -68,6 +68,11 @@ struct c2q_ctx {
     int sm_count  = 0;
     // pinned ring of the batched solvers: 4 slots x 16 right-hand sides x 4 doubles
     double* batch_ring = nullptr;
+    // device aliases of the pinned host buffers above (small solver transfers are
+    // copied by a one-block kernel through them, keeping them off the copy engines,
+    // where a large transfer of another stream would hold them up)
+    double* host_pinned_dev = nullptr;
+    double* batch_ring_dev  = nullptr;
 };
 
 struct c2q_gauge {
@@ -153,6 +158,11 @@ int tg_to_inner(c2q_ctx* ctx, const c2q_gauge* g, c2q_spinor_eo* out, const c2q_
 int tg_accumulate(c2q_ctx* ctx, const c2q_gauge* g, c2q_spinor_eo* x, c2q_spinor_eo* xs, const c2q_spinor_eo* p,
                   const SolverScalars* sc);
 int ensure_staging(c2q_ctx* ctx, size_t bytes);
+// Small copies (multiples of 4 bytes) between device memory and the device alias
+// of a pinned host buffer, by a one-block kernel on the context's stream:
+// `height` rows of `width` bytes, rows `dpitch` / `spitch` bytes apart.
+int pinned_copy(c2q_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                int height = 1);
 int ensure_partials(c2q_ctx* ctx, size_t blocks);
 
 template <int P>

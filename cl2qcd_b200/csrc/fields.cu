@@ -191,9 +191,29 @@ int ensure_partials(c2q_ctx* ctx, size_t blocks)
     return C2Q_OK;
 }
 
+__global__ void pinned_copy_kernel(const unsigned* __restrict__ src, size_t spitch, unsigned* __restrict__ dst,
+                                   size_t dpitch, int width, int height)
+{
+    for (int r = blockIdx.x; r < height; r += gridDim.x)
+        for (int c = threadIdx.x; c < width; c += blockDim.x) dst[(size_t)r * dpitch + c] = src[(size_t)r * spitch + c];
+}
+
+int pinned_copy(c2q_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, int height)
+{
+    if (width % 4 || dpitch % 4 || spitch % 4 || height < 1) return fail(ctx, C2Q_BAD_ARG, "pinned_copy: word sizes");
+    const int blocks = height < 16 ? height : 16;
+    pinned_copy_kernel<<<blocks, 32, 0, ctx->stream>>>(static_cast<const unsigned*>(src), spitch / 4,
+                                                       static_cast<unsigned*>(dst), dpitch / 4, (int)(width / 4),
+                                                       height);
+    ctx->launches++;
+    C2Q_CUDA(ctx, cudaGetLastError());
+    return C2Q_OK;
+}
+
 int read_scalars(c2q_ctx* ctx, const double* dev, int n, double* host)
 {
-    C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, dev, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    int rc = pinned_copy(ctx, ctx->host_pinned_dev, 0, dev, 0, n * sizeof(double));
+    if (rc) return rc;
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     memcpy(host, ctx->host_pinned, n * sizeof(double));
     return C2Q_OK;
@@ -704,6 +724,8 @@ C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream)
     chk(cudaMalloc(&ctx->red_result, 8 * sizeof(double)), "cudaMalloc(result)");
     chk(cudaMalloc(&ctx->scalars, sizeof(SolverScalars)), "cudaMalloc(scalars)");
     chk(cudaMallocHost(&ctx->host_pinned, 64 * sizeof(double)), "cudaMallocHost");
+    if (rc == C2Q_OK) chk(cudaHostGetDevicePointer((void**)&ctx->host_pinned_dev, ctx->host_pinned, 0),
+                          "cudaHostGetDevicePointer");
     chk(cudaEventCreate(&ctx->ev0), "cudaEventCreate");
     chk(cudaEventCreate(&ctx->ev1), "cudaEventCreate");
     for (auto& e : ctx->ring_ev) chk(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
@@ -917,9 +939,10 @@ C2Q_EXPORT int c2q_spinor_eo_destroy(c2q_spinor_eo* f)
 }
 
 static int aos_transfer(c2q_spinor_eo* f, double* host_dst, const double* host_src, int mode, int par,
-                        const double* dev_src_full)
+                        const double* dev_src_full, cudaStream_t stream = nullptr)
 {
     c2q_ctx* ctx       = f->ctx;
+    cudaStream_t st    = stream ? stream : ctx->stream;
     const size_t sites = mode == 0 ? (size_t)f->geom.seo : (size_t)f->geom.seo * 2;
     const size_t bytes = sites * 24 * sizeof(double);
     AosArgs A;
@@ -935,21 +958,21 @@ static int aos_transfer(c2q_spinor_eo* f, double* host_dst, const double* host_s
         if (host_src) {
             int rc = ensure_staging(ctx, bytes);
             if (rc) return rc;
-            C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->staging, host_src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+            C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->staging, host_src, bytes, cudaMemcpyHostToDevice, st));
             A.aos = static_cast<double*>(ctx->staging);
         } else {
             A.aos = const_cast<double*>(dev_src_full);
         }
-        aos_to_soa_kernel<<<blocks, 256, 0, ctx->stream>>>(A);
+        aos_to_soa_kernel<<<blocks, 256, 0, st>>>(A);
         ctx->launches++;
         C2Q_CUDA(ctx, cudaGetLastError());
     } else {
         A.aos = static_cast<double*>(ctx->staging);
-        soa_to_aos_kernel<<<blocks, 256, 0, ctx->stream>>>(A);
+        soa_to_aos_kernel<<<blocks, 256, 0, st>>>(A);
         ctx->launches++;
         C2Q_CUDA(ctx, cudaGetLastError());
         if (host_dst) {
-            C2Q_CUDA(ctx, cudaMemcpyAsync(host_dst, ctx->staging, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+            C2Q_CUDA(ctx, cudaMemcpyAsync(host_dst, ctx->staging, bytes, cudaMemcpyDeviceToHost, st));
         }
     }
     return C2Q_OK;
@@ -996,23 +1019,26 @@ C2Q_EXPORT int c2q_spinor_eo_download(const c2q_spinor_eo* f, double* aos)
     return C2Q_OK;
 }
 
-// The same transfers, enqueued on the context's stream without waiting (FP64
-// fields): a caller driving several contexts overlaps one context's copies with
-// another's solve.
-C2Q_EXPORT int c2q_spinor_eo_upload_async(c2q_spinor_eo* f, const double* aos)
+// The same transfers, enqueued without waiting (FP64 fields) on the context's
+// stream or on a stream of the caller's: with a copy stream the transfers of
+// one solve's source and solution overlap another solve of the same context.
+// The context's staging buffer is shared: its transfers must be ordered (one
+// stream, or events).
+C2Q_EXPORT int c2q_spinor_eo_upload_async(c2q_spinor_eo* f, const double* aos, void* stream)
 {
     if (!f || !aos) return C2Q_BAD_ARG;
     if (f->prec != 64) return fail(f->ctx, C2Q_BAD_ARG, "asynchronous transfers take FP64 fields");
-    return aos_transfer(f, nullptr, aos, 0, 0, nullptr);
+    const int rc = ensure_staging(f->ctx, (size_t)f->geom.seo * 24 * sizeof(double));
+    return rc ? rc : aos_transfer(f, nullptr, aos, 0, 0, nullptr, static_cast<cudaStream_t>(stream));
 }
 
-C2Q_EXPORT int c2q_spinor_eo_download_async(const c2q_spinor_eo* f, double* aos)
+C2Q_EXPORT int c2q_spinor_eo_download_async(const c2q_spinor_eo* f, double* aos, void* stream)
 {
     if (!f || !aos) return C2Q_BAD_ARG;
     c2q_spinor_eo* ff = const_cast<c2q_spinor_eo*>(f);
     if (f->prec != 64) return fail(f->ctx, C2Q_BAD_ARG, "asynchronous transfers take FP64 fields");
     const int rc = ensure_staging(ff->ctx, (size_t)f->geom.seo * 24 * sizeof(double));
-    return rc ? rc : aos_transfer(ff, aos, nullptr, 0, 0, nullptr);
+    return rc ? rc : aos_transfer(ff, aos, nullptr, 0, 0, nullptr, static_cast<cudaStream_t>(stream));
 }
 
 C2Q_EXPORT int c2q_spinor_eo_precision(const c2q_spinor_eo* f) { return f ? f->prec : C2Q_BAD_ARG; }

@@ -59,8 +59,8 @@ struct SolveClock {
 
 int read_sc(c2q_ctx* ctx, SolverScalars* h)
 {
-    C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, ctx->scalars, sizeof(SolverScalars), cudaMemcpyDeviceToHost,
-                                  ctx->stream));
+    int rc = pinned_copy(ctx, ctx->host_pinned_dev, 0, ctx->scalars, 0, sizeof(SolverScalars));
+    if (rc) return rc;
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     memcpy(h, ctx->host_pinned, sizeof(SolverScalars));
     return C2Q_OK;
@@ -69,8 +69,8 @@ int read_sc(c2q_ctx* ctx, SolverScalars* h)
 int write_sc(c2q_ctx* ctx, const SolverScalars& h)
 {
     memcpy(ctx->host_pinned, &h, sizeof(SolverScalars));
-    C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->scalars, ctx->host_pinned, sizeof(SolverScalars), cudaMemcpyHostToDevice,
-                                  ctx->stream));
+    int rc = pinned_copy(ctx, ctx->scalars, 0, ctx->host_pinned_dev, 0, sizeof(SolverScalars));
+    if (rc) return rc;
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return C2Q_OK;
 }
@@ -189,11 +189,10 @@ struct ResidRing {
     explicit ResidRing(c2q_ctx* c) : ctx(c) {}
     int push(int k)
     {
-        double* slot = ctx->host_pinned + 32 + 2 * (k % N);
-        C2Q_CUDA(ctx, cudaMemcpyAsync(slot, &ctx->scalars->resid, sizeof(double), cudaMemcpyDeviceToHost,
-                                      ctx->stream));
-        C2Q_CUDA(ctx, cudaMemcpyAsync(slot + 1, &ctx->scalars->flag, sizeof(int), cudaMemcpyDeviceToHost,
-                                      ctx->stream));
+        double* dslot = ctx->host_pinned_dev + 32 + 2 * (k % N);
+        int rc        = pinned_copy(ctx, dslot, 0, &ctx->scalars->resid, 0, sizeof(double));
+        if (!rc) rc = pinned_copy(ctx, dslot + 1, 0, &ctx->scalars->flag, 0, sizeof(int));
+        if (rc) return rc;
         C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[k % N], ctx->stream));
         return C2Q_OK;
     }
@@ -523,20 +522,23 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         ~Free() { cudaFreeAsync(q, c->stream); }
     } free_dsc{ctx, dsc};
     C2Q_CUDA(ctx, cudaMemsetAsync(dsc, 0, n * sizeof(SolverScalars), ctx->stream));
-    if (!ctx->batch_ring) C2Q_CUDA(ctx, cudaMallocHost(&ctx->batch_ring, 4 * PK_MAX_RHS * 4 * sizeof(double)));
+    if (!ctx->batch_ring) {
+        C2Q_CUDA(ctx, cudaMallocHost(&ctx->batch_ring, 4 * PK_MAX_RHS * 4 * sizeof(double)));
+        C2Q_CUDA(ctx, cudaHostGetDevicePointer((void**)&ctx->batch_ring_dev, ctx->batch_ring, 0));
+    }
     const double delta = P->reliable_delta > 0 ? P->reliable_delta : 0.1;
     SolveClock clock(ctx);
 
     auto write_one = [&](int k, const SolverScalars& h) -> int {
         memcpy(ctx->host_pinned, &h, sizeof(SolverScalars));
-        C2Q_CUDA(ctx, cudaMemcpyAsync(dsc + k, ctx->host_pinned, sizeof(SolverScalars), cudaMemcpyHostToDevice,
-                                      ctx->stream));
+        const int rc1 = pinned_copy(ctx, dsc + k, 0, ctx->host_pinned_dev, 0, sizeof(SolverScalars));
+        if (rc1) return rc1;
         C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         return C2Q_OK;
     };
     auto read_one = [&](int k, SolverScalars* h) -> int {
-        C2Q_CUDA(ctx, cudaMemcpyAsync(ctx->host_pinned, dsc + k, sizeof(SolverScalars), cudaMemcpyDeviceToHost,
-                                      ctx->stream));
+        const int rc1 = pinned_copy(ctx, ctx->host_pinned_dev, 0, dsc + k, 0, sizeof(SolverScalars));
+        if (rc1) return rc1;
         C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         memcpy(h, ctx->host_pinned, sizeof(SolverScalars));
         return C2Q_OK;
@@ -673,9 +675,9 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
             if (rc) return rc;
         }
         for (int k : act) S[k].sweeps += per_apply;
-        double* slot = ctx->batch_ring + (size_t)(iter % 4) * PK_MAX_RHS * 4;
-        C2Q_CUDA(ctx, cudaMemcpy2DAsync(slot, 4 * sizeof(double), &dsc[0].resid, sizeof(SolverScalars),
-                                        4 * sizeof(double), n, cudaMemcpyDeviceToHost, ctx->stream));
+        rc = pinned_copy(ctx, ctx->batch_ring_dev + (size_t)(iter % 4) * PK_MAX_RHS * 4, 4 * sizeof(double),
+                         &dsc[0].resid, sizeof(SolverScalars), 4 * sizeof(double), n);
+        if (rc) return rc;
         C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[iter % 4], ctx->stream));
         if (iter == 0) continue;
         C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[(iter - 1) % 4]));

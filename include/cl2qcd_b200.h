@@ -178,12 +178,15 @@ C2Q_EXPORT int c2q_spinor_eo_destroy(c2q_spinor_eo* f);
 C2Q_EXPORT int c2q_spinor_eo_upload(c2q_spinor_eo* f, const double* aos);
 C2Q_EXPORT int c2q_spinor_eo_download(const c2q_spinor_eo* f, double* aos);
 /* (no counterpart in the reference: its Spinor::load / dump wait) The same
- * transfers enqueued on the context's stream without waiting, FP64 fields only.
- * The host array must stay valid, and a download's must not be read, until the
- * stream has passed the copy (c2q_ctx_synchronize); with pinned host memory the
- * copy overlaps work of other contexts on the GPU. */
-C2Q_EXPORT int c2q_spinor_eo_upload_async(c2q_spinor_eo* f, const double* aos);
-C2Q_EXPORT int c2q_spinor_eo_download_async(const c2q_spinor_eo* f, double* aos);
+ * transfers enqueued without waiting, FP64 fields only, on `stream` (a
+ * cudaStream_t of the same device; NULL: the context's stream).  The host array
+ * must stay valid, and a download's must not be read, until the stream has
+ * passed the copy.  With pinned host memory and a copy stream ordered against
+ * the context's stream by events, the transfers of one solve overlap another
+ * solve.  The context's transfers share one staging buffer: keep them on one
+ * stream (or order them by events). */
+C2Q_EXPORT int c2q_spinor_eo_upload_async(c2q_spinor_eo* f, const double* aos, void* stream);
+C2Q_EXPORT int c2q_spinor_eo_download_async(const c2q_spinor_eo* f, double* aos, void* stream);
 /* Spinorfield_eo::zero / cold (physics/lattices/spinorfield_eo.cpp:147-165) */
 C2Q_EXPORT int c2q_spinor_eo_zero(c2q_spinor_eo* f);
 C2Q_EXPORT int c2q_spinor_eo_cold(c2q_spinor_eo* f);

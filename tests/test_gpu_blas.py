@@ -1,4 +1,6 @@
 """GPU parity of the eo BLAS, reductions, tm site-diagonal ops and layout conversions."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -93,19 +95,28 @@ def test_bad_arguments_raise(env, system):
 
 
 def test_async_transfers_round_trip(system, port):
-    """c2q_spinor_eo_upload_async / download_async: enqueued without waiting, the
-    data arrive after the context synchronises; FP32 fields are refused."""
+    """c2q_spinor_eo_upload_async / download_async: enqueued without waiting, on the
+    context's stream or on a copy stream of the caller's; the data arrive after
+    that stream synchronises; FP32 fields are refused."""
+    import torch
     import cl2qcd_b200 as c2q
     lib = system.lib
     L = c2q.Lattice(4, 8)
     port.set_lattice(4, 8)
     a = np.ascontiguousarray(port.pseudo_randomize(L.seo, 5))
     f = c2q.Spinorfield_eo(system, L)
-    assert lib.c2q_spinor_eo_upload_async(f.h, a) == 0
+    assert lib.c2q_spinor_eo_upload_async(f.h, a, None) == 0
     out = np.zeros_like(a)
-    assert lib.c2q_spinor_eo_download_async(f.h, out) == 0
+    assert lib.c2q_spinor_eo_download_async(f.h, out, None) == 0
     system.synchronize()
     assert np.array_equal(out, a)
+    copy = torch.cuda.Stream()
+    b = np.ascontiguousarray(port.pseudo_randomize(L.seo, 6))
+    assert lib.c2q_spinor_eo_upload_async(f.h, b, C.c_void_p(copy.cuda_stream)) == 0
+    out2 = np.zeros_like(b)
+    assert lib.c2q_spinor_eo_download_async(f.h, out2, C.c_void_p(copy.cuda_stream)) == 0
+    copy.synchronize()
+    assert np.array_equal(out2, b)
     g = c2q.Spinorfield_eo(system, L, a, precision=32)
-    assert lib.c2q_spinor_eo_upload_async(g.h, a) != 0
-    assert lib.c2q_spinor_eo_download_async(g.h, out) != 0
+    assert lib.c2q_spinor_eo_upload_async(g.h, a, None) != 0
+    assert lib.c2q_spinor_eo_download_async(g.h, out, None) != 0
