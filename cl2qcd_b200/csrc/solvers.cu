@@ -570,7 +570,8 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         }
         if (rc) return rc;
         s.resid = s.r2;
-        if (s.r2 < s.thr) {
+        // r = 0 (a zero source with a zero start): x is exact and alpha would be 0/0
+        if (s.r2 < s.thr || s.r2 == 0.0) {
             s.status       = 0;
             s.r2_confirmed = s.r2;
             continue;

@@ -117,3 +117,34 @@ def test_multi_rejects_aliasing(system):
     with pytest.raises(c2q.InvalidParameters):
         c2q.host.cg_multi([x, x], c2q.host.QplusQminus_eo(), gf, [b, b], c2q.SolverParameters(precision=16),
                           c2q.AdditionalParameters(0.15, 0.003))
+
+
+@pytest.mark.parametrize("precision", [32, 16])
+def test_zero_source_in_batch(port, system, O, precision):
+    """A zero source in a batch is solved exactly by x = 0 without iterating (alpha would be 0/0);
+    the other right-hand sides iterate as if solved alone.  The FP64 CG keeps the reference's
+    behaviour on a zero source (a stuck solver, physics/algorithms/solvers/cg.cpp:93-119)."""
+    import cl2qcd_b200 as c2q
+    L, g, gf = _problem(port, c2q, system)
+    kappa, mubar = 0.15, 2 * 0.15 * 0.01
+    add = c2q.AdditionalParameters(kappa, mubar)
+    A = c2q.host.QplusQminus_eo()
+    srcs = [c2q.host.generate_source(L.seo, "gaussian", 200), np.zeros((L.seo, 24)),
+            c2q.host.generate_source(L.seo, "z2", 201)]
+    bs = [c2q.Spinorfield_eo(system, L, s) for s in srcs]
+    xs = [c2q.Spinorfield_eo(system, L) for _ in srcs]
+    reps = []
+    its = c2q.host.cg_multi(xs, A, gf, bs, _params(c2q, precision, graph=True), add, reps)
+    assert its[1] == 0 and reps[1]["status"] == 0 and reps[1]["true_resid_rel"] == 0.0
+    assert not np.any(xs[1].dump())
+    for k in (0, 2):
+        assert reps[k]["true_resid_rel"] <= 1e-10, (k, reps[k])
+        x1 = c2q.Spinorfield_eo(system, L)
+        rep1 = {}
+        c2q.host.cg(x1, A, gf, bs[k], _params(c2q, precision), add, rep1)
+        assert rep1["iterations"] == reps[k]["iterations"]
+    x0 = c2q.Spinorfield_eo(system, L)
+    c2q.host.cg(x0, A, gf, bs[1], _params(c2q, precision), add)
+    assert not np.any(x0.dump())
+    with pytest.raises(c2q.SolverStuck):
+        c2q.host.cg(x0, A, gf, bs[1], c2q.SolverParameters(solver="cg", prec=1e-22, cgmax=50), add)

@@ -215,3 +215,16 @@ def test_oracle_reproduces_inverter_integration_reference(request, O, kind):
     C *= (2 * kappa) ** 2 / (ns * ns * nt)
     np.testing.assert_allclose(C, ref["ps_correlator"], rtol=ref["tolerance_percent"] / 100)
     np.testing.assert_allclose(C, ref["ps_correlator"], rtol=1e-9)  # far inside the reference's tolerance
+
+
+def test_oracle_cg_zero_source_is_stuck(port, O):
+    """A zero source with a zero start: the reference's CG forms alpha = (r, r) / (p, A p) = 0/0
+    in its first iteration and reports the NaN residual as a stuck solver
+    (physics/algorithms/solvers/cg.cpp:93-119)."""
+    port.set_lattice(4, 4, 1.0, 0.0)
+    g = np.zeros((4 * port.vol, 18))
+    port.lib.c2qo_fill_gauge(g, 4 * port.vol, 0)
+    b = np.zeros_like(port.pseudo_randomize(port.seo, 5))
+    x = np.zeros_like(b)
+    it = port.cg(x, O.OP_QPQM_EO, b, g, 0.12, 0.02, params=O.SolverParams(prec=1e-20, cgmax=50, solver=1))
+    assert it == O.SOLVER_STUCK
