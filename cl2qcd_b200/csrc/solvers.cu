@@ -1,6 +1,7 @@
 // solvers.cu -- CG (FP64 and mixed precision with FP64 reliable updates),
 // BiCGStab (fast and save variants) and the eo Schur-complement inversion,
 // on top of the fused sweeps of fields.cu.
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -780,9 +781,10 @@ struct EoSpace {
     Fields F;
     c2q_spinor_eo *t1 = nullptr, *t2 = nullptr;
     int sweeps = 0;
+    int prec   = 64;  // storage precision of the work fields (gk must match)
     int alloc(int n, std::vector<V>& out)
     {
-        int rc = make_fields(ctx, *lat, 64, n + 2, F, 0);
+        int rc = make_fields(ctx, *lat, prec, n + 2, F, 0);
         if (rc) return rc;
         out.resize(n);
         for (int k = 0; k < n; ++k) out[k] = &F.f[k];
@@ -1048,6 +1050,93 @@ int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, co
     return bicgstab_generic(sp, x, const_cast<c2q_spinor_eo*>(b), P, rep);
 }
 
+// Mixed-precision BiCGStab (no counterpart in the reference, whose solvers run
+// in FP64): defect correction around the BiCGStab above.  Each outer step forms
+// the true residual r = b - A x in FP64, solves A e = r / |r| by BiCGStab on
+// FP32 or FP16 fields and links until that inner residual has dropped by
+// reliable_delta (or by what the stopping test still needs), and adds |r| e to x
+// in FP64.  The stopping test (prec / rel_tol) is applied to the FP64 true
+// residual; cgmax bounds the inner iterations of all steps together.
+template <int PB>
+int bicgstab_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b,
+                   double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
+{
+    const auto t0  = std::chrono::steady_clock::now();
+    const int gk64 = P->use_rec12 ? G64R12 : G64;
+    const int gk   = gkind_for(PB, P->use_rec12);
+    int rc         = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
+    if (!rc) rc = gauge_ensure(const_cast<c2q_gauge*>(g), gk64);
+    if (rc) return rc;
+    Fields F64, FB;
+    rc = make_fields(ctx, x->lat, 64, 4, F64, 0);
+    if (!rc) rc = make_fields(ctx, x->lat, PB, 2, FB, 0);
+    if (rc) return rc;
+    c2q_spinor_eo *r64 = &F64.f[0], *a64 = &F64.f[1], *b64 = &F64.f[2], *e64 = &F64.f[3];
+    c2q_spinor_eo *rin = &FB.f[0], *ein = &FB.f[1];
+    double b2 = 0;
+    rc        = norm2(ctx, b, &b2);
+    if (rc) return rc;
+    const double thr   = stop_threshold(P, b2);
+    const double delta = P->reliable_delta > 0 && P->reliable_delta < 1 ? P->reliable_delta : 0.003;
+    c2q_solver_params in = *P;
+    in.rel_tol           = 0.0;
+    in.min_iter          = 0;
+    int iters = 0, steps = 0, sweeps = 0, status = C2Q_DID_NOT_SOLVE;
+    double r2 = 0;
+    for (;;) {
+        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, gk64);
+        if (rc) return rc;
+        if (r2 != r2) {
+            status = C2Q_SOLVER_STUCK;
+            break;
+        }
+        if (r2 < thr || r2 == 0.0) {
+            status = iters;
+            break;
+        }
+        if (iters >= P->cgmax) break;
+        const double rn = std::sqrt(r2);
+        BlasSpec sc;  // a64 = r / |r|, then to the inner precision
+        sc.op  = B_SAX;
+        sc.out = a64;
+        sc.x   = r64;
+        sc.a   = coef_host(1.0 / rn, 0.0);
+        rc     = launch_blas(ctx, sc);
+        if (!rc) rc = launch_convert(ctx, rin, a64);
+        if (!rc) rc = c2q_spinor_eo_zero(ein);
+        if (rc) return rc;
+        in.cgmax = P->cgmax - iters;
+        in.prec  = std::max(delta * delta, 0.01 * thr / r2);
+        EoSpace sp{ctx, &x->lat, op, g, gk, kappa, mubar, action};
+        sp.prec = PB;
+        c2q_solve_report ir{};
+        const int st = bicgstab_generic(sp, ein, rin, &in, &ir);
+        if (st < 0 && st != C2Q_SOLVER_STUCK && st != C2Q_DID_NOT_SOLVE) return st;
+        sweeps += sp.sweeps;
+        iters += ir.iterations;
+        ++steps;
+        if (st == C2Q_SOLVER_STUCK && ir.iterations == 0) {
+            status = C2Q_SOLVER_STUCK;
+            break;
+        }
+        BlasSpec up;  // x += |r| e in FP64
+        up.op  = B_SAXPY;
+        up.out = x;
+        up.x   = e64;
+        up.y   = x;
+        up.a   = coef_host(-rn, 0.0);
+        rc     = launch_convert(ctx, e64, ein);
+        if (!rc) rc = launch_blas(ctx, up);
+        if (rc) return rc;
+    }
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    finish_report(rep, status, iters, steps, r2, b2 > 0 ? std::sqrt(r2 / b2) : 0.0, secs, sweeps);
+    if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
+    if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "mixed-precision BiCGStab stuck (NaN residual or vanishing rho)");
+    return status;
+}
+
 // CG with host-side scalars, physics/algorithms/solvers/cg.cpp:277-400: the
 // residual is refreshed every iter_refresh iterations and checked every
 // resid_check_every (|r|^2 < prec; with rel_tol confirmed by the true
@@ -1177,7 +1266,11 @@ C2Q_EXPORT int c2q_bicgstab(c2q_spinor_eo* x, int op, const c2q_gauge* g, const 
     int rc       = 0;
     if (!validate(ctx, x, g, b, p, &rc)) return rc;
     if (x == b) return fail(ctx, C2Q_BAD_ARG, "solution and source must be different fields");
-    return bicgstab_impl(ctx, x, op, g, b, kappa, mubar, action, p, report);
+    switch (p->precision) {
+        case 64: return bicgstab_impl(ctx, x, op, g, b, kappa, mubar, action, p, report);
+        case 32: return bicgstab_mixed<32>(ctx, x, op, g, b, kappa, mubar, action, p, report);
+        default: return bicgstab_mixed<16>(ctx, x, op, g, b, kappa, mubar, action, p, report);
+    }
 }
 
 C2Q_EXPORT int c2q_cg_multi(c2q_spinor_eo* const* x, int op, const c2q_gauge* g, const c2q_spinor_eo* const* b,

@@ -71,6 +71,31 @@ def test_bicgstab_matches_oracle(port, system, O, variant):
     assert rel_l2(X.dump(), x_ref) < 1e-8
 
 
+@pytest.mark.parametrize("variant", ["bicgstab", "bicgstab_save"])
+@pytest.mark.parametrize("precision", [32, 16])
+@pytest.mark.parametrize("opname", ["Aee", "Qminus_eo"])
+def test_mixed_bicgstab_true_residual(port, system, O, variant, precision, opname):
+    """Mixed-precision BiCGStab (inner BiCGStab on FP32 / FP16 fields, FP64 defect correction)
+    reaches ||b - A x|| / ||b|| <= 1e-10, checked with the oracle operator, and agrees with the
+    solution of the oracle's FP64 BiCGStab."""
+    import cl2qcd_b200 as c2q
+    L, g, gf, b = _prob(port, c2q, system, 8, 4)
+    kappa, mubar = 0.13, 2 * 0.13 * 0.05
+    opc = {"Aee": O.OP_AEE, "Qminus_eo": O.OP_QMINUS_EO}[opname]
+    X, B = c2q.Spinorfield_eo(system, L), c2q.Spinorfield_eo(system, L, b)
+    rep = {}
+    it = c2q.host.bicgstab(X, getattr(c2q.host, opname)(), gf, B,
+                           c2q.SolverParameters(solver=variant, prec=0.0, rel_tol=1e-10, cgmax=5000,
+                                                precision=precision), c2q.AdditionalParameters(kappa, mubar), rep)
+    assert it > 0 and rep["reliable_updates"] >= 2, rep
+    assert rep["true_resid_rel"] <= 1e-10, rep
+    r = port.apply(opc, X.dump(), g, kappa, mubar)
+    assert np.linalg.norm(r - b) / np.linalg.norm(b) <= 1.5e-10
+    x_ref = np.zeros_like(b)
+    assert port.bicgstab(x_ref, opc, b, g, kappa, mubar, params=O.SolverParams(prec=1e-20, cgmax=5000)) > 0
+    assert rel_l2(X.dump(), x_ref) < 1e-8
+
+
 @pytest.mark.parametrize("precision", [64, 32, 16])
 @pytest.mark.parametrize("rec12", [False, True])
 def test_cg_true_residual_1e10(port, system, O, precision, rec12):
@@ -151,6 +176,24 @@ def test_perform_inversion_matches_oracle(port, system, O, solver):
                                          c2q.AdditionalParameters(kappa, mubar))
     assert rel_l2(out, ref) < 1e-9
     # the reference's eo inversion returns -M^{-1} b
+    assert rel_l2(port.m_tm_plus(-out, g, kappa, mubar), src) < 1e-9
+
+
+@pytest.mark.parametrize("precision", [32, 16])
+def test_perform_inversion_mixed_bicgstab(port, system, O, precision):
+    """perform_inversion with the reference's default solver (bicgstab) in mixed precision."""
+    import cl2qcd_b200 as c2q
+    port.set_lattice(4, 8, 1.0, 0.0)
+    L = c2q.Lattice(4, 8, 1.0, 0.0)
+    g = c2q.host.generate_gaugefield(L, 0.25, 4)
+    gf = c2q.Gaugefield(system, L, g)
+    src = c2q.host.generate_source(port.vol, "gaussian", 5)
+    kappa, mubar = 0.14, 2 * 0.14 * 0.05
+    ref, _, _ = port.perform_inversion_eo(src, g, kappa, mubar, params=O.SolverParams(prec=1e-22, cgmax=2000))
+    out, it = c2q.host.perform_inversion(system, gf, src, c2q.SolverParameters(
+        solver="bicgstab", prec=0.0, rel_tol=1e-11, cgmax=2000, precision=precision),
+        c2q.AdditionalParameters(kappa, mubar))
+    assert rel_l2(out, ref) < 1e-9
     assert rel_l2(port.m_tm_plus(-out, g, kappa, mubar), src) < 1e-9
 
 
