@@ -48,7 +48,8 @@ struct BlasArgs {
     Coef a, b;
     int n, stride;
     int op;
-    int dot;          // 0 none, 1 <x,y> (conj(x) y, no output write), 2 |out|^2
+    int dot;          // 0 none, 1 <x,y> (conj(x) y, no output write), 2 |out|^2,
+                      // 3 <x,y> and <x,x> in one pass (no output write)
     RedArgs red;
 };
 
@@ -57,10 +58,10 @@ __global__ void __launch_bounds__(BLAS_THREADS) blas_kernel(const BlasArgs<P> A)
 {
     using R      = typename Prec<P>::R;
     const int i  = blockIdx.x * blockDim.x + threadIdx.x;
-    double dv[2] = {0.0, 0.0};
+    double dv[4] = {0.0, 0.0, 0.0, 0.0};
     if (i < A.n) {
         Cplx<R> xv[12], r[12];
-        if (A.dot == 1) {
+        if (A.dot == 1 || A.dot == 3) {
             Cplx<R> yv[12];
             SpinorIO<P>::load(A.x, A.stride, i, xv);
             SpinorIO<P>::load(A.y, A.stride, i, yv);
@@ -69,6 +70,11 @@ __global__ void __launch_bounds__(BLAS_THREADS) blas_kernel(const BlasArgs<P> A)
                 Cplx<R> p = cmulc(xv[k], yv[k]);
                 dv[0] += (double)p.re;
                 dv[1] += (double)p.im;
+                if (A.dot == 3) {  // <x,x>: its imaginary part is rounding only
+                    Cplx<R> q = cmulc(xv[k], xv[k]);
+                    dv[2] += (double)q.re;
+                    dv[3] += (double)q.im;
+                }
             }
         } else {
             const Cplx<double> a = coef_value(A.a), b = coef_value(A.b);
@@ -117,7 +123,11 @@ __global__ void __launch_bounds__(BLAS_THREADS) blas_kernel(const BlasArgs<P> A)
                 for (int k = 0; k < 12; ++k) dv[0] += (double)r[k].re * r[k].re + (double)r[k].im * r[k].im;
         }
     }
-    if (A.dot) {
+    if (A.dot == 3) {
+        __shared__ double smem4[128];
+        block_sum<4>(dv, smem4);
+        finish_reduction<4>(dv, A.red, smem4);
+    } else if (A.dot) {
         __shared__ double smem[64];
         block_sum<2>(dv, smem);
         finish_reduction<2>(dv, A.red, smem);

@@ -529,8 +529,8 @@ static int blas_typed(c2q_ctx* ctx, const BlasSpec& s, const c2q_spinor_eo* ref)
     A.op     = s.op;
     A.dot    = s.dot;
     const int blocks = (A.n + BLAS_THREADS - 1) / BLAS_THREADS;
-    if (s.dot) {
-        int rc = ensure_partials(ctx, blocks);
+    if (s.dot) {  // dot 3 reduces four doubles per block
+        int rc = ensure_partials(ctx, s.dot == 3 ? 2 * (size_t)blocks : (size_t)blocks);
         if (rc) return rc;
     }
     A.red = red_args(ctx, s.fin);

@@ -110,6 +110,22 @@ int dot_read(c2q_ctx* ctx, const c2q_spinor_eo* x, const c2q_spinor_eo* y, Cx* o
     return rc;
 }
 
+// <x,y> and <x,x> in one pass over x and y (read back together)
+int dot2_read(c2q_ctx* ctx, const c2q_spinor_eo* x, const c2q_spinor_eo* y, Cx* xy, Cx* xx)
+{
+    BlasSpec s;
+    s.x    = x;
+    s.y    = y;
+    s.dot  = 3;
+    int rc = launch_blas(ctx, s);
+    if (rc) return rc;
+    double h[4];
+    rc  = read_scalars(ctx, ctx->red_result, 4, h);
+    *xy = {h[0], h[1]};
+    *xx = {h[2], h[3]};
+    return rc;
+}
+
 int copy_field(c2q_ctx* ctx, c2q_spinor_eo* to, const c2q_spinor_eo* from)
 {
     BlasSpec s;
@@ -821,6 +837,7 @@ struct EoSpace {
     int copy(V to, V from) { return copy_field(ctx, to, from); }
     int zero(V f) { return c2q_spinor_eo_zero(f); }
     int dot(V x, V y, Cx* out) { return dot_read(ctx, x, y, out); }
+    int dot2(V x, V y, Cx* xy, Cx* xx) { return dot2_read(ctx, x, y, xy, xx); }
 };
 
 struct FullSpace {
@@ -875,6 +892,15 @@ struct FullSpace {
         int rc = dot_read(ctx, x.e, y.e, &a);
         if (!rc) rc = dot_read(ctx, x.o, y.o, &b);
         *out = {a.re + b.re, a.im + b.im};
+        return rc;
+    }
+    int dot2(V x, V y, Cx* xy, Cx* xx)
+    {
+        Cx a{0, 0}, b{0, 0}, c{0, 0}, d{0, 0};
+        int rc = dot2_read(ctx, x.e, y.e, &a, &c);
+        if (!rc) rc = dot2_read(ctx, x.o, y.o, &b, &d);
+        *xy = {a.re + b.re, a.im + b.im};
+        *xx = {c.re + d.re, c.im + d.im};
         return rc;
     }
 };
@@ -959,8 +985,7 @@ int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_p
             alpha = cdiv(rho, tmp1);
             rc    = sp.saxpy(s, alpha, v, rn);
             if (!rc) rc = sp.apply(t, s);
-            if (!rc) rc = sp.dot(t, s, &tmp1);
-            if (!rc) rc = sp.dot(t, t, &tmp2);
+            if (!rc) rc = sp.dot2(t, s, &tmp1, &tmp2);  // (t, s) and (t, t)
             if (rc) return rc;
             omega = cdiv(tmp1, tmp2);
             rc    = sp.saxsbypz(x, alpha, p, omega, s, x);
@@ -1012,8 +1037,7 @@ int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_p
             alpha = cdiv(rho, tmp1);
             rc    = sp.saxpy(s, alpha, v, rn);
             if (!rc) rc = sp.apply(t, s);
-            if (!rc) rc = sp.dot(t, s, &tmp1);
-            if (!rc) rc = sp.dot(t, t, &tmp2);
+            if (!rc) rc = sp.dot2(t, s, &tmp1, &tmp2);  // (t, s) and (t, t)
             if (rc) return rc;
             omega = cdiv(tmp1, tmp2);
             rc    = sp.saxpy(rn, omega, t, s);
