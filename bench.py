@@ -35,12 +35,34 @@ NS, NT = 32, 64
 EPS, KAPPA, MU = 0.25, 0.16, 0.005
 GAUGE_SEED, SOURCE_SEED = 20250, 777
 REL_TOL = 1e-10
-# FP64 CG iterations this workload needs to reach 1e-10 (the reference's CG is the
-# same algorithm in FP64); used to scale the CPU reference's per-iteration sample
-# to solves/s when the GPU arm is not run in the same process.
-FP64_CG_ITERATIONS = 91  # measured on B200 by this bench (fp64.iterations_reference_semantics)
+# The FP64 CG iterations the reference's CG (on its own kernels, with its stopping
+# test |r|^2 < REL_TOL^2 |b|^2) performed on this workload, recorded by one full
+# CPU solve (oracle/record_workload.py); the CPU arm times a bounded sample of
+# those iterations and scales by this count.
+WORKLOAD_RECORD = os.path.join(ROOT, "oracle", "workload_fp64_cg.json")
 WORKLOAD = (f"32^3x64 tm-Wilson eo CG on QplusQminus_eo, 1 gaussian source, kappa {KAPPA}, mu {MU}, "
             f"eps {EPS}, antiperiodic T, x0 = 0, true residual {REL_TOL}")
+
+
+def bench_config(ws, precision=16):
+    """The `config` of the JSON line, the same for the GPU and the reference arm."""
+    return {"workload": WORKLOAD, "lattice": "32x32x32x64", "global_batch": ws,
+            "inner_precision": precision, "links": "12-real", "parallelism": f"replicas x{ws}",
+            "l2": "inputs larger than L2 (FP16 12-real links 201 MB, FP64 links 1.2 GB)"}
+
+
+def recorded_fp64_iterations():
+    """(iterations, record) of the reference's FP64 CG on this workload, or (None, why)."""
+    try:
+        with open(WORKLOAD_RECORD) as f:
+            rec = json.load(f)
+    except OSError as e:
+        return None, f"no recorded FP64 iteration count ({e.strerror})"
+    w = rec["workload"]
+    if (w["ns"], w["nt"], w["eps"], w["kappa"], w["mu"], w["gauge_seed"], w["source_seed"], w["rel_tol"]) != \
+            (NS, NT, EPS, KAPPA, MU, GAUGE_SEED, SOURCE_SEED, REL_TOL):
+        return None, "the recorded FP64 iteration count is for another workload"
+    return int(rec["iterations"]), rec
 
 
 def parse():
@@ -180,7 +202,8 @@ def cpu_reference_sample(g, b, fp64_iters, budget_s=15.0):
     solves = 1.0 / (per_iter * fp64_iters)
     return {"value": solves, "unit": "solves/s", "cores": threads, "kind": kind,
             "sample": f"{n} FP64 CG iterations (+1 refresh) of this 32^3x64 workload on the reference's kernels "
-                      f"in {tn:.1f} s, scaled by {fp64_iters} FP64 iterations per solve",
+                      f"in {tn:.1f} s; solves/s = 1 / (seconds per iteration x {fp64_iters}), the iterations the "
+                      f"reference's CG performed in a full solve of this workload (oracle/workload_fp64_cg.json)",
             "seconds_per_iteration": per_iter}
 
 
@@ -190,7 +213,6 @@ def cpu_reference_extras(g, b, budget_s=10.0):
     (8^4, eps 0.3, kappa 0.15, mu 0.01, one Z2 source) solved to a true residual
     1e-10 by the reference CG on its own kernels."""
     import oracle as O
-    import cl2qcd_b200 as c2q
     kind = "reference" if O.available("reference") else "port"
     o = O.Oracle(kind)
     o.set_lattice(NS, NT, 1.0, 0.0)
@@ -201,8 +223,8 @@ def cpu_reference_extras(g, b, budget_s=10.0):
         n += 1
     t = time.perf_counter() - t0
     gbs = DSLASH_BYTES[(64, 0)] * b.shape[0] * n / t / 1e9
-    c1 = config1_inputs(c2q)
     o.set_lattice(8, 8, 1.0, 0.0)
+    c1 = {"g": o.gauge_generate(8, 8, 0.3, 1), "b": o.source_generate(o.seo, "z2", 2)}
     b2 = float((c1["b"] ** 2).sum())
     P = O.SolverParams(prec=REL_TOL ** 2 * b2, cgmax=10000, solver=1)
     x = np.zeros_like(c1["b"])
@@ -216,6 +238,24 @@ def cpu_reference_extras(g, b, budget_s=10.0):
     o.set_lattice(NS, NT, 1.0, 0.0)
     return {"dslash_gbs": round(gbs, 2), "dslash_sample": f"{n} FP64 18-real dslash_eo sweeps of 32^3x64",
             "config1_solves_per_s": round(m / t1, 2), "config1_sample": f"{m} solves of 8^4 to 1e-10"}
+
+
+def oracle_check(g, b, x, ms_precision):
+    """The benchmark's final mixed-precision solution checked by the oracle:
+    ||b - A x|| / ||b|| recomputed on the host by the reference's own kernels
+    with the 18-real FP64 links as generated (outside every timed region)."""
+    import oracle as O
+    kind = "reference" if O.available("reference") else "port"
+    o = O.Oracle(kind)
+    o.set_lattice(NS, NT, 1.0, 0.0)
+    t0 = time.perf_counter()
+    r = o.apply(O.OP_QPQM_EO, x, g, KAPPA, mbar())
+    r -= b
+    rel = float(np.linalg.norm(r) / np.linalg.norm(b))
+    return {"true_resid_rel": rel, "pass": rel <= REL_TOL * (1 + 1e-6), "oracle": kind,
+            "operator": "QplusQminus_eo on the 18-real FP64 links as generated",
+            "solution": f"the last timed mixed-precision (FP{ms_precision} inner) solve",
+            "seconds": round(time.perf_counter() - t0, 2)}
 
 
 def config1_inputs(c2q):
@@ -419,23 +459,27 @@ def inputs():
 def run_reference(args, budget_s=150.0):
     """The reference arm: the reference's own kernels (oracle/_ref, compiled from
     the reference sources; the restatement if they are absent) running the
-    reference CG on this workload on the host cores.  args.warmup untimed and
-    args.steps timed steps; each step is one CG call of a bounded number of
-    iterations, sized so the whole run takes about budget_s; solves/s scales the
-    measured time per iteration by the FP64 iteration count of a solve.  Under
-    torchrun only rank 0 runs."""
+    reference CG on this workload on the host cores, with the workload's inputs
+    from the oracle's own generators (bit-identical to the library's; the
+    library is not loaded).  args.warmup untimed and args.steps timed steps;
+    each step is one CG call of a bounded number of iterations, sized so the
+    whole run takes about budget_s; solves/s scales the measured time per
+    iteration by the iteration count the reference's CG needed for a full solve
+    of this workload (recorded by oracle/record_workload.py).  Under torchrun
+    only rank 0 runs."""
     ws, rank, local = dist_env()
     if rank != 0:
         return 0
-    lat, g, b = inputs()
-    iters = FP64_CG_ITERATIONS
+    iters, rec = recorded_fp64_iterations()
     if iters is None:
-        print(json.dumps({"impl": "reference", "unavailable": "FP64 iteration count of the workload not recorded"}))
+        print(json.dumps({"impl": "reference", "unavailable": rec}))
         return 0
     import oracle as O
     kind = "reference" if O.available("reference") else "port"
     o = O.Oracle(kind)
     o.set_lattice(NS, NT, 1.0, 0.0)
+    g = o.gauge_generate(NS, NT, EPS, GAUGE_SEED)
+    b = o.source_generate(o.seo, "gaussian", SOURCE_SEED)
     threads = int(os.environ.get("OMP_NUM_THREADS", "0")) or os.cpu_count()
     x = np.zeros_like(b)
 
@@ -457,12 +501,15 @@ def run_reference(args, budget_s=150.0):
     per_iter = t / (steps * (n + 1))
     value = 1.0 / (per_iter * iters)
     sample = (f"{steps} steps of {n} FP64 CG iterations (+1 refresh) of this 32^3x64 workload on the "
-              f"{'reference' if kind == 'reference' else 'restated'} kernels, {threads} threads, "
-              f"{t:.1f} s, scaled by {iters} FP64 iterations per solve")
+              f"{'reference' if kind == 'reference' else 'restated'} kernels, {threads} threads, {t:.1f} s; "
+              f"solves/s = 1 / (seconds per iteration x {iters}), the iterations the reference's CG performed "
+              f"in a full solve of this workload ({rec['seconds']} s on {rec['threads']} threads, true residual "
+              f"{rec['true_resid_rel']:.2e}, oracle/workload_fp64_cg.json)")
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": steps,
             "warmup": warmup, "ms_per_step": t / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "lattice": "32x32x32x64"},
+            "config": bench_config(ws),
+            "extrapolation": {"measured": f"{steps * (n + 1)} iterations", "scaled_to": f"{iters} iterations"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -772,9 +819,15 @@ def main():
     serving = serving_run(c2q, [1.0], args.serve_requests) if rank == 0 and ws == 1 else None
 
     cpu_baseline = None
+    rec_iters, _rec = recorded_fp64_iterations()
+    check = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            cpu_baseline = cpu_reference_sample(g, b, ref_iters)
+            check = oracle_check(g, b, xm, args.precision)
+        except Exception as e:  # reported, never required
+            check = {"error": repr(e)}
+        try:
+            cpu_baseline = cpu_reference_sample(g, b, rec_iters or ref_iters)
             cpu_baseline.pop("seconds_per_iteration", None)
             cpu_baseline.update(cpu_reference_extras(g, b))
         except Exception as e:  # the baseline is reported, never required
@@ -790,9 +843,7 @@ def main():
             "dtype": {16: "f16-fixed-point storage, f32 arithmetic, f64 reliable updates",
                       32: "f32 inner, f64 reliable updates", 64: "f64"}[args.precision],
             "data": "synthetic: seeded U=exp(i*0.25*H) gauge field (reunitarised in f64), gaussian source",
-            "config": {"workload": WORKLOAD, "lattice": "32x32x32x64", "global_batch": ws,
-                       "inner_precision": args.precision, "links": "12-real", "parallelism": f"replicas x{ws}",
-                       "l2": "inputs larger than L2 (FP16 12-real links 201 MB, FP64 links 1.2 GB)"},
+            "config": bench_config(ws, args.precision),
             "e2e": {"value": ws * args.steps / te, "unit": "solves/s", "h2d_bytes_per_step": lat.seo * 24 * 8,
                     "d2h_bytes_per_step": lat.seo * 24 * 8,
                     "mode": "public API, pinned host buffers; every step uploads its source and downloads its "
@@ -813,8 +864,10 @@ def main():
             "mixed": {"iterations": it_m, "reliable_updates": [r["reliable_updates"] for r in reps],
                       "true_resid_rel": max(r["true_resid_rel"] for r in reps),
                       "rel_err_vs_fp64_solution": err_vs_fp64},
+            "oracle_check": check,
             "fp64": {"solves_per_s": 1.0 / fp64_s, "iterations": rep64["iterations"],
                      "iterations_reference_semantics": ref_iters,
+                     "iterations_reference_cg_on_cpu": rec_iters,
                      "true_resid_rel": rep64["true_resid_rel"], "seconds": fp64_s},
             "fp32_inner": {"solves_per_s": 1.0 / fp32_s, "iterations": rep32["iterations"],
                            "reliable_updates": rep32["reliable_updates"], "true_resid_rel": rep32["true_resid_rel"]},

@@ -89,6 +89,8 @@ SIGNATURES = {
     "c2q_gauge_download": (C.c_int, [_P, _D]),
     "c2q_gauge_destroy": (C.c_int, [_P]),
     "c2q_gauge_device_bytes": (C.c_size_t, [_P]),
+    "c2q_gauge_unitarity": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "c2q_gauge_reunitarize": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "c2q_spinor_eo_create": (C.c_int, [_P, C.POINTER(CLattice), C.POINTER(_P)]),
     "c2q_spinor_eo_create_precision": (C.c_int, [_P, C.POINTER(CLattice), C.c_int, C.POINTER(_P)]),
     "c2q_spinor_eo_precision": (C.c_int, [_P]),

@@ -86,6 +86,8 @@ struct c2q_gauge {
     // and the weight of the T hop leaving the last time slice
     c2q::GaugeStore tg_transform;
     double tg_lam_re = 1.0, tg_lam_im = 0.0;
+    // max |row 2 - conj(row0 x row1)| of the uploaded links (-1: not measured yet)
+    double rec12_dev = -1.0;
 };
 
 struct c2q_spinor_eo {
@@ -140,6 +142,17 @@ int field_alloc(c2q_ctx* ctx, const c2q_lattice& lat, int prec, c2q_spinor_eo* f
 void field_free(c2q_spinor_eo* f);
 size_t field_bytes(const Geom& g, int prec);
 int gauge_ensure(c2q_gauge* g, int kind);  // builds a lower-precision copy on first use
+// frees every copy derived from the FP64 18-real links (rebuilt on next use)
+int gauge_drop_derived(c2q_gauge* g);
+// 12-real FP64 links are the same operator as the uploaded 18-real ones when
+// row 2 of every link equals conj(row0 x row1) to this tolerance (unitarity.cu)
+constexpr double REC12_EXACT_TOL = 1e-13;
+bool rec12_exact(c2q_gauge* g);
+// the FP64 links a solver's residuals use: 12-real only where they are the same operator
+inline int gk64_for(const c2q_gauge* g, int rec12)
+{
+    return rec12 && rec12_exact(const_cast<c2q_gauge*>(g)) ? G64R12 : G64;
+}
 
 // ---- temporal gauge (tgauge.cu) ----
 // The inner solves of the mixed-precision CG may run on the field transformed

@@ -399,6 +399,19 @@ int gauge_ensure(c2q_gauge* g, int kind)
     return C2Q_OK;
 }
 
+int gauge_drop_derived(c2q_gauge* g)
+{
+    c2q_ctx* ctx = g->ctx;
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int k = 1; k < GAUGE_KINDS; ++k) {
+        cudaFree(g->store[k].data);
+        g->store[k] = GaugeStore{};
+    }
+    cudaFree(g->tg_transform.data);
+    g->tg_transform = GaugeStore{};
+    return C2Q_OK;
+}
+
 // ------------------------------------------------------------------ launches
 template <int P, int NL, int EPI, int DOT, int PH>
 static void dslash_go(const DslashParams<P>& prm, int blocks, cudaStream_t s)
@@ -879,13 +892,9 @@ C2Q_EXPORT int c2q_gauge_upload(c2q_gauge* g, const double* aos)
     C2Q_CUDA(ctx, cudaGetLastError());
     // lower-precision copies (and the temporal gauge) are rebuilt from the new
     // links on next use
-    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    for (int k = 1; k < GAUGE_KINDS; ++k) {
-        cudaFree(g->store[k].data);
-        g->store[k] = GaugeStore{};
-    }
-    cudaFree(g->tg_transform.data);
-    g->tg_transform = GaugeStore{};
+    rc = gauge_drop_derived(g);
+    if (rc) return rc;
+    g->rec12_dev = -1.0;
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return C2Q_OK;
 }

@@ -254,6 +254,9 @@ C2Q_EXPORT int c2q_server_add_gauge(c2q_server* s, unsigned long long gauge_id, 
     // so that solves running side by side only read the gauge object
     if (!rc && gkind_tg(inner) >= 0 && tg_applicable(g->lat)) rc = gauge_ensure(g, gkind_tg(inner));
     if (!rc && s->rec12) rc = gauge_ensure(g, G64R12);
+    // whether 12-real FP64 residuals are exact for this field, measured here
+    // (once) rather than by the first solve that asks
+    if (!rc && s->rec12) (void)rec12_exact(g);
     if (!rc) rc = c2q_ctx_synchronize(s->loader);
     if (rc) {
         if (g) c2q_gauge_destroy(g);

@@ -234,7 +234,9 @@ int cg_fp64(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2
     int rc = make_fields(ctx, x->lat, 64, 5, F, 0);
     if (rc) return rc;
     c2q_spinor_eo *p = &F.f[0], *rn = &F.f[1], *v = &F.f[2], *t1 = &F.f[3], *t2 = &F.f[4];
-    const int gk = gkind_for(64, P->use_rec12);
+    // 12-real links when asked for and the field is SU(3) to rounding (the final
+    // true residual always uses the links as uploaded)
+    const int gk = gk64_for(g, P->use_rec12);
     int sweeps   = 0;
     SolveClock clock(ctx);
 
@@ -525,9 +527,11 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
     // residuals enter as G r, increments leave as G^dagger x_s
     const bool use_tg = op == C2Q_OP_QPLUSQMINUS_EO && P->use_temporal_gauge && tg_applicable(lat);
     const int gk      = use_tg ? gkind_tg(gkind_for(PB, P->use_rec12)) : gkind_for(PB, P->use_rec12);
-    // FP64 true residuals on 12-real FP64 links when 12-real links were asked
-    // for (row 2 rebuilt in FP64: the operator agrees to rounding)
-    const int gk64 = P->use_rec12 ? G64R12 : G64;
+    // FP64 residuals of the intermediate reliable updates on 12-real FP64 links
+    // when 12-real links were asked for and the uploaded field is SU(3) to
+    // rounding (row 2 rebuilt in FP64: the same operator); the residual that
+    // decides convergence, and the one reported, always use the links as uploaded
+    const int gk64 = gk64_for(g, P->use_rec12);
     rc             = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
     if (!rc) rc = gauge_ensure(const_cast<c2q_gauge*>(g), gk64);
     if (rc) return rc;
@@ -582,7 +586,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
             rc   = to_inner(rs[k], b[k]);
             s.r2 = s.b2;
         } else {
-            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, gk64);
+            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, G64);
             if (!rc) rc = to_inner(rs[k], r64);
         }
         if (rc) return rc;
@@ -719,11 +723,18 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
             if (rn > s.maxrr) s.maxrr = rn;
             if (rn < delta * s.maxrr || resid < s.thr) {
                 // reliable update in FP64 after iteration `iter`
+                // (an update expected to be the last one uses the uploaded links;
+                // one that converges unexpectedly on 12-real links is confirmed on them)
                 SolverScalars h;
                 rc = read_one(k, &h);
                 if (!rc) rc = take_out(k, fused ? nullptr : dsc + k);
+                const int gk_upd = resid < s.thr ? G64 : gk64;
                 if (!rc)
-                    rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps, gk64);
+                    rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps,
+                                       gk_upd);
+                if (!rc && gk_upd != G64 && s.r2 < s.thr)
+                    rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps,
+                                       G64);
                 if (rc) return rc;
                 ++s.reliable;
                 s.resid = s.r2;
@@ -765,7 +776,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         RhsState& s = S[k];
         double r2t  = s.r2_confirmed;
         if (r2t < 0) {
-            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &r2t, &s.sweeps, gk64);
+            rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &r2t, &s.sweeps, G64);
             if (rc) return rc;
         }
         finish_report(reps ? &reps[k] : nullptr, s.status, s.iters, s.reliable, s.resid,
@@ -1071,7 +1082,7 @@ int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_p
 int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b,
                   double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
 {
-    EoSpace sp{ctx, &x->lat, op, g, gkind_for(64, P->use_rec12), kappa, mubar, action};
+    EoSpace sp{ctx, &x->lat, op, g, gk64_for(g, P->use_rec12), kappa, mubar, action};
     return bicgstab_generic(sp, x, const_cast<c2q_spinor_eo*>(b), P, rep);
 }
 
@@ -1087,7 +1098,9 @@ int bicgstab_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, c
                    double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
 {
     const auto t0  = std::chrono::steady_clock::now();
-    const int gk64 = P->use_rec12 ? G64R12 : G64;
+    // 12-real FP64 residuals only where they are the uploaded operator; the
+    // residual that stops the solve is confirmed on the links as uploaded
+    const int gk64 = gk64_for(g, P->use_rec12);
     const int gk   = gkind_for(PB, P->use_rec12);
     int rc         = gauge_ensure(const_cast<c2q_gauge*>(g), gk);
     if (!rc) rc = gauge_ensure(const_cast<c2q_gauge*>(g), gk64);
@@ -1110,6 +1123,8 @@ int bicgstab_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, c
     double r2 = 0;
     for (;;) {
         rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, gk64);
+        if (!rc && gk64 != G64 && r2 < thr)
+            rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, G64);
         if (rc) return rc;
         if (r2 != r2) {
             status = C2Q_SOLVER_STUCK;

@@ -175,6 +175,21 @@ class Gaugefield:
     def device_bytes(self):
         return self.system.lib.c2q_gauge_device_bytes(self.h)
 
+    def unitarity(self) -> dict:
+        """FP64 distance of the uploaded links from SU(3), measured on the device:
+        max |U U^dagger - 1| (entry-wise), max |det U - 1|, and max |row 2 -
+        conj(row0 x row1)| (what 12-real storage changes)."""
+        dev = (C.c_double * 3)()
+        _check(self.system.lib.c2q_gauge_unitarity(self.h, dev), self.system.h, self.system.lib)
+        return {"unitarity": dev[0], "det": dev[1], "rec12": dev[2]}
+
+    def reunitarize(self) -> float:
+        """project_su3 (ocl_kernel/operations_gaugefield.cl:135-240) on every link
+        in FP64 on the device; returns max |U U^dagger - 1| before the projection."""
+        before = C.c_double()
+        _check(self.system.lib.c2q_gauge_reunitarize(self.h, C.byref(before)), self.system.h, self.system.lib)
+        return before.value
+
     def _destroy(self):
         # a context outlives its objects: nothing to do once the context is closed
         if getattr(self, "h", None) and getattr(self.system, "h", None):

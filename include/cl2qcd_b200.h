@@ -136,6 +136,64 @@ typedef struct {
     double dslash_applications; /* dslash launches (each = one parity sweep over the lattice) */
 } c2q_solve_report;
 
+/* ---------------- input parameters ----------------
+ * The reference's input-file keys of the inverter path (meta::Inputparameters,
+ * meta/inputparameters.cpp:150-196, read by boost's parse_config_file):
+ *   nSpace, nTime, precision, useReconstruct12, startCondition, initialConf,
+ *   ignoreChecksumErrors (meta/parametersConfig.cpp:147-187);
+ *   fermionAction, kappa, mu, thetaFermionSpatial/Temporal,
+ *   useChemicalPotentialRe/Im, chemicalPotentialRe/Im, useEO,
+ *   useKernelMergingFermionMatrix/Spinor (meta/parametersFermion.cpp:106-150);
+ *   solver, solverPrecision, solverMaxIterations, solverMinIterations,
+ *   solverRestartEvery, solverResiduumCheckEvery (meta/parametersSolver.cpp:74-107);
+ *   sourceType, sourceContent, nSources, sourceX/Y/Z/T
+ *   (meta/parametersSources.cpp:67-90); measureCorrelators,
+ *   correlatorDirection (meta/parametersObs.cpp:67-86);
+ * with the aliases NS, NT, use_evenodd, ThetaT, ThetaS
+ * (meta/inputparameters.cpp:180-193) and mubar = 2 kappa mu (meta/util.cpp:56-59).
+ * Keys of this library, without a counterpart in the reference, sit in the
+ * section [b200]: innerPrecision (64, 32, 16), relativeTolerance,
+ * reliableDelta, useGraph, temporalGauge. */
+#define C2Q_START_COLD 0      /* startCondition cold / cold_start */
+#define C2Q_START_HOT 1       /* hot / hot_start */
+#define C2Q_START_CONTINUE 2  /* continue / source / start_from_source */
+#define C2Q_SOURCE_POINT 0    /* sourceType (common::sourcetypes) */
+#define C2Q_SOURCE_VOLUME 1
+#define C2Q_SOURCE_TIMESLICE 2
+#define C2Q_SOURCE_ZSLICE 3
+#define C2Q_CONTENT_ONE 0     /* sourceContent (common::sourcecontents) */
+#define C2Q_CONTENT_Z4 1
+#define C2Q_CONTENT_GAUSSIAN 2
+#define C2Q_CONTENT_Z2 3
+typedef struct {
+    c2q_lattice lat;              /* nSpace, nTime, thetaFermion*, chemical potential */
+    int fermion_action;           /* fermionAction: C2Q_ACTION_WILSON or C2Q_ACTION_TWISTEDMASS */
+    double kappa, mu;             /* kappa, mu */
+    double mubar;                 /* 2 kappa mu */
+    int use_eo;                   /* useEO */
+    int precision;                /* precision (64) */
+    int use_merge_kernels_fermion, use_merge_kernels_spinor;
+    c2q_solver_params solver;     /* solver keys; use_rec12 = useReconstruct12; [b200] keys */
+    int start_condition;          /* C2Q_START_* */
+    char initial_conf[1024];      /* initialConf */
+    int ignore_checksum_errors;   /* ignoreChecksumErrors */
+    int source_type, source_content, n_sources;
+    int source_pos[4];            /* sourceX, sourceY, sourceZ, sourceT */
+    int measure_correlators;      /* measureCorrelators */
+    int correlator_direction;     /* correlatorDirection (0 or 3) */
+} c2q_params;
+/* The reference's defaults (the constructors of meta/parameters*.cpp). */
+C2Q_EXPORT void c2q_params_default(c2q_params* p);
+/* Parses input-file text onto p (start from c2q_params_default; a second call
+ * overrides what the first set, as the reference's command-line options
+ * override its input file).  Format of parse_config_file: `name = value` per
+ * line, `#` comments, `[section]` headers; unknown names and a name given twice
+ * are errors; every other key the reference defines (HMC, RHMC, gauge, I/O) is
+ * accepted and ignored.  Returns C2Q_OK, or C2Q_BAD_ARG with p unchanged and the
+ * reason in c2q_params_last_error() (per thread). */
+C2Q_EXPORT int c2q_params_from_kv(const char* key_value_text, c2q_params* p);
+C2Q_EXPORT const char* c2q_params_last_error(void);
+
 /* ---------------- context ---------------- */
 /* Creates a context on `device`.  `cuda_stream` (a cudaStream_t) is borrowed
  * if non-NULL, else the context creates its own.  Replaces hardware::System /
@@ -169,6 +227,22 @@ C2Q_EXPORT int c2q_gauge_download(const c2q_gauge* g, double* aos);
 C2Q_EXPORT int c2q_gauge_destroy(c2q_gauge* g);
 /* Device bytes held by the gauge object (all precisions built so far). */
 C2Q_EXPORT size_t c2q_gauge_device_bytes(const c2q_gauge* g);
+/* FP64 unitarity of the uploaded links, measured on the device (no
+ * counterpart in the reference, which takes SU(3) for granted wherever it
+ * reconstructs a link): dev[0] = max over links of max_ij |(U U^dagger - 1)_ij|,
+ * dev[1] = max |det U - 1|, dev[2] = max_j |U_2j - conj(row0 x row1)_j| (what
+ * 12-real storage changes).  Non-finite links give infinity.  The solvers use
+ * 12-real FP64 links for intermediate residuals only when dev[2] <= 1e-13; the
+ * residual that stops a mixed-precision solve, and every reported true
+ * residual, use the links as uploaded. */
+C2Q_EXPORT int c2q_gauge_unitarity(const c2q_gauge* g, double* dev);
+/* project_su3 (ocl_kernel/operations_gaugefield.cl:135-240; applied by the
+ * reference after every link update, md_update_gaugefield.cl:44) on every link,
+ * in FP64 on the device, in place: column 0 normalised, column 1
+ * orthogonalised against it and normalised, column 2 = conj(col0 x col1).
+ * dev_before (may be NULL) receives c2q_gauge_unitarity's dev[0] before the
+ * projection.  Copies derived from the links are rebuilt on next use. */
+C2Q_EXPORT int c2q_gauge_reunitarize(c2q_gauge* g, double* dev_before);
 
 /* ---------------- eo spinor fields ---------------- */
 /* physics::lattices::Spinorfield_eo (physics/lattices/spinorfield_eo.hpp:48-305). */

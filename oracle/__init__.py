@@ -108,6 +108,8 @@ class Oracle:
             "c2qo_fill_gauge": (None, [_D, sz, i]),
             "c2qo_fill_ascending_complex": (None, [_D, sz]),
             "c2qo_count_sf": (d, [_D, sz]),
+            "c2qo_gauge_generate": (i, [_D, i, i, d, C.c_ulonglong]),
+            "c2qo_source_generate": (i, [_D, sz, i, C.c_ulonglong]),
         }
         for fn, (res, args) in sig.items():
             f = getattr(L, fn)
@@ -284,6 +286,21 @@ class Oracle:
 
     def count_sf(self, a):
         return self.lib.c2qo_count_sf(np.ascontiguousarray(a), a.shape[0])
+
+    # ---- the workload's seeded inputs (oracle_inputs.c) ----
+    def gauge_generate(self, ns, nt, eps, seed):
+        """U = exp(i eps H) per link, Matrixsu3[4V] (4*ns^3*nt, 18)."""
+        g = np.empty((4 * ns ** 3 * nt, 18))
+        if self.lib.c2qo_gauge_generate(g, ns, nt, eps, seed) != 0:
+            raise ValueError("bad gauge generator arguments")
+        return g
+
+    def source_generate(self, n_sites, kind, seed):
+        """kind "z2" or "gaussian": (n_sites, 24)."""
+        out = np.empty((n_sites, 24))
+        if self.lib.c2qo_source_generate(out, n_sites, {"z2": 0, "gaussian": 1}[kind], seed) != 0:
+            raise ValueError("bad source generator arguments")
+        return out
 
 
 def available(kind: str) -> bool:
