@@ -37,6 +37,17 @@ class CSolverParams(C.Structure):
                 ("use_graph", C.c_int), ("use_temporal_gauge", C.c_int)]
 
 
+class CParams(C.Structure):
+    """c2q_params: the reference's inverter input keys (c2q_params_from_kv)."""
+    _fields_ = [("lat", CLattice), ("fermion_action", C.c_int), ("kappa", C.c_double), ("mu", C.c_double),
+                ("mubar", C.c_double), ("use_eo", C.c_int), ("precision", C.c_int),
+                ("use_merge_kernels_fermion", C.c_int), ("use_merge_kernels_spinor", C.c_int),
+                ("solver", CSolverParams), ("start_condition", C.c_int), ("initial_conf", C.c_char * 1024),
+                ("ignore_checksum_errors", C.c_int), ("source_type", C.c_int), ("source_content", C.c_int),
+                ("n_sources", C.c_int), ("source_pos", C.c_int * 4), ("measure_correlators", C.c_int),
+                ("correlator_direction", C.c_int)]
+
+
 class CSolveReport(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("reliable_updates", C.c_int),
                 ("resid_sq", C.c_double), ("true_resid_rel", C.c_double), ("seconds", C.c_double),
@@ -76,6 +87,9 @@ _P = C.c_void_p
 # name -> (restype, argtypes); the declarations of include/cl2qcd_b200.h
 SIGNATURES = {
     "c2q_version": (C.c_char_p, []),
+    "c2q_params_default": (None, [C.POINTER(CParams)]),
+    "c2q_params_from_kv": (C.c_int, [C.c_char_p, C.POINTER(CParams)]),
+    "c2q_params_last_error": (C.c_char_p, []),
     "c2q_ctx_create": (C.c_int, [C.POINTER(_P), C.c_int, _P]),
     "c2q_ctx_destroy": (C.c_int, [_P]),
     "c2q_last_error": (C.c_char_p, [_P]),

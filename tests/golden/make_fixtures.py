@@ -22,6 +22,7 @@ reference tree and the oracle built; the fixtures themselves are committed).
    inputs, used to pin the restated oracle and the CUDA path.
 
 Usage:  python tests/golden/make_fixtures.py [/path/to/reference]
+        (default: the directory named by the environment variable CL2QCD_REFERENCE)
 """
 from __future__ import annotations
 
@@ -145,12 +146,13 @@ def extract_kats(ref: str) -> dict:
     for name, inp in (("inverter_test_ref", "inverter_test_input_1"), ("inverter_test_ref2", "inverter_test_input_2")):
         vals = _floats(open(os.path.join(ref, "executables/tests", name)).read())
         params = {}
-        for line in open(os.path.join(ref, "executables/tests", inp)):
+        text = open(os.path.join(ref, "executables/tests", inp)).read()
+        for line in text.splitlines():
             if "=" in line:
                 k, v = line.strip().split("=", 1)
                 params[k] = v
-        out["inverter"][name] = {"ps_correlator": vals, "input": params, "tolerance_percent": 0.1,
-                                 "where": f"executables/tests/{name}, {inp}"}
+        out["inverter"][name] = {"ps_correlator": vals, "input": params, "input_text": text,
+                                 "tolerance_percent": 0.1, "where": f"executables/tests/{name}, {inp}"}
     return out
 
 
@@ -187,7 +189,9 @@ def decode_conf00200(ref: str) -> dict:
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CL2QCD_REFERENCE", "")
+    if not ref or not os.path.isdir(ref):
+        raise SystemExit("name the reference tree: make_fixtures.py /path/to/reference, or set CL2QCD_REFERENCE")
     kats = extract_kats(ref)
     kats["ildg_conf00200"] = decode_conf00200(ref)
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:

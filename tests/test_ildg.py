@@ -103,9 +103,10 @@ def test_conf00200_fixture():
 
 
 def test_reader_on_reference_file():
-    path = "/root/reference/ildg_io/conf.00200"
-    if not os.path.exists(path):
-        pytest.skip("reference tree not present")
+    ref = os.environ.get("CL2QCD_REFERENCE", "")
+    path = os.path.join(ref, "ildg_io", "conf.00200")
+    if not ref or not os.path.exists(path):
+        pytest.skip("reference tree not named by CL2QCD_REFERENCE, or absent")
     import cl2qcd_b200 as c2q
     ns, nt, aos, info = c2q.host.read_ildg(path)
     assert np.array_equal(aos, CONF["gauge"]) and info["checksum_status"] == 1
