@@ -97,7 +97,10 @@ C2Q_EXPORT int c2q_ildg_read(const char* path, double* aos, size_t aos_len, int*
         char type[129];
         memcpy(type, h + 16, 128);
         type[128] = 0;
-        if (off + 144 + len > file.size()) return C2Q_BAD_ARG;  // truncated
+        // truncated record (off + 144 <= size holds; compared this way a length
+        // read from a damaged header cannot wrap around), or a length whose
+        // 8-byte padding would not fit a size_t
+        if (len > file.size() - off - 144 || len > SIZE_MAX - 7) return C2Q_BAD_ARG;
         const unsigned char* payload = h + 144;
         const std::string t(type);
         if (t == "ildg-format") format.assign(reinterpret_cast<const char*>(payload), len);

@@ -21,6 +21,7 @@
 // ticket is cleared on the caller's stream before each launch, and calls
 // whose work overlaps on the GPU (different streams, or several host threads
 // on one device) race on the array and give wrong results.
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -69,6 +70,12 @@ C2Q_EXPORT int c2q_scalar_product_eo_noalloc(const void* x_soa, const void* y_so
                                              double* result_dev, void* cuda_stream)
 {
     if (!x_soa || !y_soa || !result_dev || n_sites <= 0 || stride < n_sites) return C2Q_BAD_ARG;
+    // the kernel reads the fields as double2 and writes two doubles: refuse
+    // pointers it could not use (a misaligned view) before anything launches
+    if ((((uintptr_t)x_soa | (uintptr_t)y_soa) & 15u) || ((uintptr_t)result_dev & 7u)) {
+        fprintf(stderr, "c2q_scalar_product_eo_noalloc: x and y must be 16-byte aligned, result 8-byte aligned\n");
+        return C2Q_BAD_ARG;
+    }
     if (n_sites > C2Q_NOALLOC_MAX_SITES) {
         fprintf(stderr,
                 "c2q_scalar_product_eo_noalloc: %d sites exceed the fixed scratch of this entry point "

@@ -352,9 +352,13 @@ C2Q_EXPORT int c2q_saxpy_AND_squarenorm(c2q_spinor_eo* out, double alpha_re, dou
  * Allocates nothing: the reduction scratch is a fixed array inside the library
  * (about 256 KiB per device, held until the process exits); more than
  * C2Q_NOALLOC_MAX_SITES sites is rejected with C2Q_BAD_ARG (and a message on
- * stderr).  The first call on a device looks up the scratch's device address,
- * so make that call before any stream capture.  Calls share the scratch:
- * calls that overlap on the GPU (other streams or host threads) race. */
+ * stderr), and so are x_soa / y_soa not 16-byte aligned or result_dev not
+ * 8-byte aligned.  The first call on a device looks up the scratch's device
+ * address, so make that call before any stream capture; the address is kept
+ * for the life of the process, so a process that resets a device
+ * (cudaDeviceReset) must not call this entry point on it afterwards.  Calls
+ * share the scratch: calls that overlap on the GPU (other streams or host
+ * threads) race. */
 #define C2Q_NOALLOC_MAX_SITES 4194304
 C2Q_EXPORT int c2q_scalar_product_eo_noalloc(const void* x_soa, const void* y_soa, int n_sites, int stride,
                                              double* result_dev, void* cuda_stream);

@@ -91,6 +91,28 @@ def test_reader_round_trip(tmp_path, prec, checksum):
     assert "plaquette = 0.5" in info["xlf_info"]
 
 
+@pytest.mark.parametrize("damage", ["truncated", "huge_length", "wrapping_length"])
+def test_reader_rejects_damaged_records(tmp_path, damage):
+    """A record whose header claims more bytes than the file holds -- cut off,
+    absurdly long, or long enough to wrap a 64-bit offset -- is refused."""
+    import cl2qcd_b200 as c2q
+    ns, nt = 4, 4
+    V = ns ** 3 * nt
+    links = np.ones((V, 4, 3, 3), dtype=complex)
+    path = str(tmp_path / "cfg.lime")
+    _write_ildg(path, links, ns, nt, 64, "good")
+    raw = bytearray(open(path, "rb").read())
+    if damage == "truncated":
+        raw = raw[:len(raw) - 4000]
+    else:  # the length field of the first record (bytes 8..16 of its header)
+        n = (1 << 62) if damage == "huge_length" else (1 << 64) - 100
+        raw[8:16] = struct.pack(">Q", n)
+    bad = str(tmp_path / "bad.lime")
+    open(bad, "wb").write(bytes(raw))
+    with pytest.raises(Exception):
+        c2q.host.read_ildg(bad)
+
+
 def test_conf00200_fixture():
     import cl2qcd_b200 as c2q
     meta = KATS["ildg_conf00200"]

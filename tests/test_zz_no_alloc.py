@@ -67,3 +67,8 @@ def test_noalloc_rejects_oversized_fields(lib):
     dummy = torch.zeros(2, dtype=torch.float64, device="cuda")
     p = C.c_void_p(dummy.data_ptr())
     assert lib.c2q_scalar_product_eo_noalloc(p, p, n, n, p, None) == -5  # C2Q_BAD_ARG, nothing launched
+    # misaligned caller buffers (a view at an odd offset) are refused before any launch
+    base = dummy.data_ptr()
+    assert lib.c2q_scalar_product_eo_noalloc(C.c_void_p(base + 8), p, 64, 64, p, None) == -5
+    assert lib.c2q_scalar_product_eo_noalloc(p, C.c_void_p(base + 8), 64, 64, p, None) == -5
+    assert lib.c2q_scalar_product_eo_noalloc(p, p, 64, 64, C.c_void_p(base + 4), None) == -5
