@@ -156,6 +156,155 @@ def extract_kats(ref: str) -> dict:
     return out
 
 
+def _extents(tok):
+    m = re.search(r"LatticeExtents\{ns(\d+),\s*nt(\d+)\}", tok)
+    return int(m.group(1)), int(m.group(2))
+
+
+def _num(expr, ntp):
+    return float(eval(expr.replace("nonTrivialParameter", repr(ntp)).replace(".*", "*")))
+
+
+def _cases(src, suites):
+    """(suite, case, call text) of every BOOST_AUTO_TEST_CASE inside the named suites."""
+    out = []
+    for sm in re.finditer(r"BOOST_AUTO_TEST_SUITE\((\w+)\)(.*?)BOOST_AUTO_TEST_SUITE_END\(\)", src, re.S):
+        if sm.group(1) not in suites:
+            continue
+        for cm in re.finditer(r"BOOST_AUTO_TEST_CASE\((\w+)\)\s*\{(.*?)\}\s*(?=BOOST_AUTO_TEST_CASE|\Z)",
+                              sm.group(2), re.S):
+            out.append((sm.group(1), cm.group(1), " ".join(cm.group(2).split())))
+    return out
+
+
+def _reference_value_tables(src, ntp):
+    """calculateReferenceValues_<name>: list of (python condition, value per lattice site)
+    from its `if (...)` blocks returning `ReferenceValues{latticeVolume * (v)}`."""
+    tables = {}
+    for fm in re.finditer(r"calculateReferenceValues_(\w+)\([^)]*\)\s*\{(.*?)\n\}", src, re.S):
+        stack, rows = [], []
+        body = re.sub(r"\b(and|or)\s*\n\s*", r"\1 ", fm.group(2))  # conditions continued on the next line
+        for line in body.splitlines():
+            t = line.strip()
+            m = re.match(r"(\}\s*else\s+)?if \((.*)\)\s*\{$", t)
+            if m:
+                if m.group(1):
+                    stack.pop()
+                stack.append(m.group(2))
+                continue
+            m = re.match(r"return ReferenceValues\{latticeVolume \* \(([-+0-9.eE]+)\)\};", t)
+            if m:
+                rows.append((" and ".join(f"({c})" for c in stack), float(m.group(1))))
+                continue
+            if t == "}" and stack:
+                stack.pop()
+        conv = []
+        for cond, v in rows:
+            c = (cond.replace("massParameters.kappa", "kappa").replace("massParameters.mu", "mu")
+                 .replace("coefficient.re", "cre").replace("coefficient.im", "cim")
+                 .replace("GaugefieldFillType::cold", "'cold'").replace("GaugefieldFillType::nonTrivial", "'nonTrivial'")
+                 .replace("gF", "gf").replace("nonTrivialParameter", repr(ntp)))
+            conv.append((c, v))
+        tables[fm.group(1)] = conv
+    return tables
+
+
+def _lookup(table, **env):
+    for cond, v in table:
+        if eval(cond, {}, env):
+            return v
+    raise ValueError(f"no reference value for {env}")
+
+
+def extract_blas_kats(ref: str) -> dict:
+    """The eo BLAS suites of hardware/code/spinors_test.cpp, the merged kernels of
+    fermions_merged_kernels_test.cpp and spinors_merged_kernels_test.cpp.  The
+    cases (lattice, fills, coefficients, masses) are read from the test sources;
+    the expected values are the tests' own: the closed forms of spinors_test.cpp:30-106
+    (restated below) and the per-site constants of the merged-kernel tests (read
+    from their calculateReferenceValues_* functions)."""
+    ntp = float(re.search(r"nonTrivialParameter\s*=\s*([0-9.]+)",
+                          open(os.path.join(ref, "hardware/code/kernelTester.hpp")).read()).group(1))
+    sq24 = (2 * 24 ** 3 + 3 * 24 ** 2 + 24) / 6.0  # sumOfIntegersSquared(24), testUtilities.cpp:42-45
+    odd, even = float(sum(range(1, 24, 2))), float(sum(range(2, 25, 2)))  # sumOfIntegers(1,23,2), (2,24,2)
+    src = open(os.path.join(ref, "hardware/code/spinors_test.cpp")).read()
+    out = {"spinors_eo": [], "merged_eo": [], "where": "hardware/code/spinors_test.cpp, "
+           "fermions_merged_kernels_test.cpp, spinors_merged_kernels_test.cpp (tolerance 1e-9 relative, "
+           "kernelTester.cpp)", "nonTrivialParameter": ntp}
+    fills = lambda t: re.findall(r"SpinorFillType::(\w+)", t)
+    coeffs = lambda t: [[float(a), float(b)] for a, b in re.findall(r"\{\s*([-0-9.]+),\s*([-0-9.]+)\s*\}", t)]
+    for suite, case, call in _cases(src, {"GLOBAL_SQUARENORM_EO", "SCALAR_PRODUCT_EO", "ZERO_EO", "COLD_EO", "SAX_EO",
+                                          "SAXPY_EO", "SAXSBYPZ_EO", "CONVERT_EO"}):
+        fn = call.split("(")[0]
+        ns, nt = _extents(call)
+        seo = ns ** 3 * nt // 2
+        e = {"suite": suite, "case": case, "test": fn, "ns": ns, "nt": nt}
+        if fn == "testEvenOddSquarenorm":
+            f = fills(call)
+            e.update(fills=f, expect=[seo * (12.0 if f[0] == "one" else sq24)])
+        elif fn == "testEvenOddScalarProduct":
+            f = fills(call)
+            val = {("one", "one"): (12.0, 0.0), ("one", "ascendingComplex"): (odd, even),
+                   ("ascendingComplex", "one"): (odd, -even),
+                   ("ascendingComplex", "ascendingComplex"): (sq24, 0.0)}[tuple(f)]
+            e.update(fills=f, expect=[seo * val[0], seo * val[1]])
+        elif fn in ("testEvenOddZero", "testEvenOddCold"):
+            e.update(fills=fills(call), expect=[0.0 if fn == "testEvenOddZero" else 0.5])
+        elif fn in ("testEvenOddSax", "testEvenOddSaxpy", "testEvenOddSaxpyArg", "testSaxsbypzEvenOdd"):
+            c = coeffs(call.split("ComplexNumbers", 1)[1])
+            if fn == "testEvenOddSax":
+                k = complex(*c[0])
+            elif fn == "testSaxsbypzEvenOdd":
+                k = 1 + complex(*c[0]) + complex(*c[1])
+            else:
+                k = 1 - complex(*c[0])
+            e.update(fills=["ascendingComplex"], coefficients=c, expect=[abs(k) ** 2 * seo * sq24])
+        elif fn == "testConvertToEvenOdd":
+            even_sites = "true" in call
+            e.update(fill_even_sites=even_sites, expect=[12.0 * seo if even_sites else 0.0,
+                                                         0.0 if even_sites else 12.0 * seo])
+        else:
+            continue
+        out["spinors_eo"].append(e)
+    msrc = open(os.path.join(ref, "hardware/code/fermions_merged_kernels_test.cpp")).read()
+    tables = _reference_value_tables(msrc, ntp)
+    kinds = {"testDslashEvenOddAndMTmInverseSitediagonal": "dslashEvenOddAndMTmInverseSitediagonal",
+             "testDslashEvenOddAndMTmInverseSitediagonalMinus": "dslashEvenOddAndMTmInverseSitediagonalMinus",
+             "testMTmSitediagonalAndGamma5EvenOdd": "mTmSitediagonalAndGamma5EvenOdd",
+             "testMTmSitediagonalMinusAndGamma5EvenOdd": "mTmSitediagonalMinusAndGamma5EvenOdd",
+             "testSaxpyAndGamma5EvenOdd": "saxpyAndGamma5EvenOdd"}
+    for suite, case, call in _cases(msrc, {"DSLASH_AND_M_TM_INVERSE_SITEDIAGONAL_EO",
+                                           "DSLASH_AND_M_TM_INVERSE_SITEDIAGONAL_MINUS_EO",
+                                           "M_TM_SITEDIAGONAL_AND_GAMMA5_EO", "M_TM_SITEDIAGONAL_MINUS_AND_GAMMA5_EO",
+                                           "SAXPY_AND_GAMMA5_EO"}):
+        fn = call.split("(")[0]
+        ns, nt = _extents(call)
+        e = {"suite": suite, "case": case, "test": fn, "ns": ns, "nt": nt, "fills": fills(call)}
+        if fn == "testSaxpyAndGamma5EvenOdd":
+            a, b = re.search(r"hmc_complex\{([^,]+),([^}]+)\}", call).groups()
+            cre, cim = _num(a, ntp), _num(b, ntp)
+            e.update(coefficient=[cre, cim], per_site=_lookup(tables[kinds[fn]], cre=cre, cim=cim))
+        else:
+            a, b = re.search(r"TwistedMassMassParameters\{([^,]+),([^}]+)\}", call).groups()
+            kappa, mu = _num(a, ntp), _num(b, ntp)
+            gm = re.search(r"GaugefieldFillType::(\w+)", call)
+            gf = gm.group(1) if gm else None
+            e.update(kappa=kappa, mu=mu, gauge=gf,
+                     per_site=_lookup(tables[kinds[fn]], kappa=kappa, mu=mu, gf=gf))
+            if gf is not None:
+                e["evenodd"] = 1 if call.rstrip(") ;").endswith("true") else 0
+        out["merged_eo"].append(e)
+    ssrc = open(os.path.join(ref, "hardware/code/spinors_merged_kernels_test.cpp")).read()
+    for suite, case, call in _cases(ssrc, {"SF_SAXPY_AND_SQUARENORM_EO"}):
+        ns, nt = _extents(call)
+        cre, cim = [float(x) for x in re.search(r"hmc_complex\{([^,]+),([^}]+)\}", call).groups()]
+        k = 1 - complex(cre, cim)
+        out["merged_eo"].append({"suite": suite, "case": case, "test": "testSaxpyAndSquarenormEvenOdd", "ns": ns,
+                                 "nt": nt, "fills": ["ascendingComplex"], "coefficient": [cre, cim],
+                                 "expect_total": abs(k) ** 2 * (ns ** 3 * nt // 2) * sq24})
+    return out
+
+
 def make_ref_outputs(path):
     import oracle as O
     R = O.Oracle("reference")
@@ -193,6 +342,7 @@ if __name__ == "__main__":
     if not ref or not os.path.isdir(ref):
         raise SystemExit("name the reference tree: make_fixtures.py /path/to/reference, or set CL2QCD_REFERENCE")
     kats = extract_kats(ref)
+    kats["blas_and_merged_eo"] = extract_blas_kats(ref)
     kats["ildg_conf00200"] = decode_conf00200(ref)
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
         json.dump(kats, f, indent=1, sort_keys=True)
