@@ -77,8 +77,14 @@ def parse():
                     help="serving sweep only: Poisson requests at rising rates, p50/p99 latency and solves/s")
     ap.add_argument("--serve-requests", type=int, default=16)
     ap.add_argument("--serve-rates", default="0.5,1,2,4")
-    ap.add_argument("--phase", default="all", choices=["all", "mixed", "dslash", "large"],
-                    help="mixed: only the warm-up and timed mixed-precision solves (for profiling)")
+    ap.add_argument("--serve-slots", default="4",
+                    help="comma-separated slot counts; the same request list is served with each")
+    ap.add_argument("--phase", default="all", choices=["all", "mixed", "dslash", "large", "mrhs"],
+                    help="mixed: only the warm-up and timed mixed-precision solves (for profiling); "
+                         "mrhs: batched multi-RHS solves on --ns^3 x --nt (for profiling a batched sweep)")
+    ap.add_argument("--ns", type=int, default=24)
+    ap.add_argument("--nt", type=int, default=48)
+    ap.add_argument("--nrhs", type=int, default=12)
     return ap.parse_args()
 
 
@@ -389,10 +395,49 @@ def large_volume(c2q, system, e0, e1):
     return out
 
 
+def mrhs_phase(c2q, args):
+    """Profiling driver of the batched sweeps: on ns^3 x nt (default 24^3 x 48,
+    whose fields and links together exceed L2), kappa 0.16, mu 0.005, eps 0.25
+    links, nrhs spin-colour point sources solved by the mixed-precision CG with
+    FP16 inner fields, once as one batch and once one source at a time, without
+    graphs, with a fixed launch configuration (no autotuner launches); reports
+    the per-launch time of the inner sweeps of each."""
+    import torch
+    os.environ["C2Q_AUTOTUNE"] = "0"
+    system = c2q.System(0)
+    lat = c2q.Lattice(args.ns, args.nt, 1.0, 0.0)
+    gf = c2q.Gaugefield(system, lat, c2q.host.generate_gaugefield(lat, EPS, GAUGE_SEED))
+    add = c2q.AdditionalParameters(KAPPA, mbar())
+    A = c2q.host.QplusQminus_eo()
+    n = args.nrhs
+    Bs = [c2q.Spinorfield_eo(system, lat, c2q.host.point_source(lat.seo, k % 12)) for k in range(n)]
+    Xs = [c2q.Spinorfield_eo(system, lat) for _ in range(n)]
+    P = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=16, use_rec12=True)
+    out = {"lattice": f"{args.ns}^3x{args.nt}", "nrhs": n}
+    lib = system.lib
+    for label, batches in (("batch", [list(range(n))]), ("single", [[k] for k in range(n)])):
+        for x_ in Xs:
+            x_.zero()
+        lib.c2q_ctx_profile(system.h, 1)
+        t0 = time.perf_counter()
+        for bt in batches:
+            c2q.host.cg_multi([Xs[k] for k in bt], A, gf, [Bs[k] for k in bt], P, add)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        nl, ms, by = C.c_longlong(), C.c_double(), C.c_double()
+        lib.c2q_ctx_profile_read(system.h, 16, C.byref(nl), C.byref(ms), C.byref(by))
+        lib.c2q_ctx_profile(system.h, 0)
+        out[label] = {"sweeps": nl.value, "sweep_ms_total": round(ms.value, 3), "solve_wall_s": round(wall, 3),
+                      "sweep_gbs": round(by.value / (ms.value * 1e-3) / 1e9, 1) if ms.value > 0 else None}
+    out["per_rhs_sweep_time_batch_over_single"] = out["batch"]["sweep_ms_total"] / out["single"]["sweep_ms_total"]
+    system.close()
+    return out
+
+
 SERVE_VOLUMES = [(16, 32), (24, 48), (32, 64), (48, 96)]
 
 
-def serving_run(c2q, rates, n_requests, slots=4, seed=4242, log=None):
+def serving_run(c2q, rates, n_requests, slots=4, seed=4242, log=None, max_heavy=1):
     """Poisson-arriving inversion requests: volume uniform over SERVE_VOLUMES
     (one resident gauge field per volume, eps ~ U[0.2, 0.35]), kappa ~ U[0.14, 0.16],
     mu ~ U[0.002, 0.02], 1-12 Z2 sources, mixed-precision (FP16 inner) to 1e-10.
@@ -402,6 +447,7 @@ def serving_run(c2q, rates, n_requests, slots=4, seed=4242, log=None):
     p50 / p99 (nearest rank), and solves/s = sources solved / wall time."""
     rng = np.random.default_rng(seed)
     server = c2q.host.Server(0, slots=slots, precision=16)
+    server.set_heavy_limit(1 << 19, max_heavy)
     lats = []
     t_setup = time.time()
     for v, (ns, nt) in enumerate(SERVE_VOLUMES):
@@ -413,6 +459,7 @@ def serving_run(c2q, rates, n_requests, slots=4, seed=4242, log=None):
     t_setup = time.time() - t_setup
     P = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000)
     out = {"volumes": [f"{ns}^3x{nt}" for ns, nt in SERVE_VOLUMES], "slots": slots, "inner_precision": 16,
+           "heavy_requests_at_a_time": max_heavy, "heavy": "eo sites x sources >= 2^19",
            "sources": "Z2, 1-12 per request", "gauge_setup_s": round(t_setup, 1),
            "budget_bytes": server.stats()["budget_bytes"], "gauge_bytes": server.stats()["gauge_bytes"],
            "rates": []}
@@ -531,9 +578,15 @@ def main():
     if args.serve:
         if rank == 0:
             rates = [float(x) for x in args.serve_rates.split(",")]
-            res = serving_run(c2q, rates, args.serve_requests,
-                              log=lambda e: print(json.dumps({"serving_rate": e}), flush=True))
-            print(json.dumps({"metric": METRIC, "serving": res}))
+            for slots in [int(x) for x in args.serve_slots.split(",")]:
+                for max_heavy in sorted({1, slots}):
+                    res = serving_run(c2q, rates, args.serve_requests, slots=slots, max_heavy=max_heavy,
+                                      log=lambda e: print(json.dumps({"serving_rate": e}), flush=True))
+                    print(json.dumps({"metric": METRIC, "serving": res}), flush=True)
+        return 0
+    if args.phase == "mrhs":
+        if rank == 0:
+            print(json.dumps({"phase": "mrhs", "mrhs": mrhs_phase(c2q, args)}))
         return 0
     from cl2qcd_b200.replicas import Replicas
     replicas = Replicas("nccl", timeout_s=600, device=torch.device("cuda", local))

@@ -170,6 +170,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_int)]),
     "c2q_server_create": (C.c_int, [C.POINTER(_P), C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_int]),
     "c2q_server_add_gauge": (C.c_int, [_P, C.c_ulonglong, C.POINTER(CLattice), _D]),
+    "c2q_server_set_heavy_limit": (C.c_int, [_P, C.c_longlong, C.c_int]),
     "c2q_server_submit": (C.c_int, [_P, C.POINTER(CRequest), C.POINTER(C.c_longlong)]),
     "c2q_server_wait": (C.c_int, [_P, C.c_longlong, C.POINTER(CRequestResult)]),
     "c2q_server_get_stats": (C.c_int, [_P, C.POINTER(CServerStats)]),

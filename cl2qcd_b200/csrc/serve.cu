@@ -15,7 +15,12 @@
 // Admission: first fit in arrival order; once the oldest waiting request has
 // waited longer than `fairness_s` seconds, nothing may overtake it, so large
 // requests are not starved.  A request whose footprint exceeds the whole
-// budget fails with C2Q_OOM without running.
+// budget fails with C2Q_OOM without running.  A "heavy" request -- eo sites
+// times sources at least `heavy_site_rhs`, enough slots for several waves of
+// blocks on every SM -- saturates the GPU by itself: two of them side by side
+// share SMs and L2 and finish later than one after the other, so at most
+// `max_heavy` heavy requests run at a time, while light requests (launch- and
+// latency-bound) are admitted beside them.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -40,6 +45,7 @@ struct Job {
     c2q_request req{};
     c2q_request_result res{};
     size_t footprint = 0;
+    bool heavy       = false;
     bool done        = false;
 };
 
@@ -58,6 +64,9 @@ struct c2q_server {
     size_t gauge_bytes = 0;      // resident gauge fields
     size_t reserved = 0;         // footprints of running requests
     double fairness_s = 2.0;
+    long long heavy_site_rhs = 1LL << 19;  // eo sites x sources of a request that fills the GPU alone
+    int max_heavy            = 1;          // heavy requests running at a time
+    int running_heavy        = 0;
     Clock::time_point t0;
     c2q_ctx* loader = nullptr;   // builds the gauge fields
     std::mutex m;
@@ -95,7 +104,7 @@ std::shared_ptr<Job> pick(c2q_server* s)
     const double t     = s->now();
     for (size_t i = 0; i < s->queue.size(); ++i) {
         auto& j = s->queue[i];
-        if (j->footprint <= avail) {
+        if (j->footprint <= avail && (!j->heavy || s->running_heavy < s->max_heavy)) {
             auto out = j;
             s->queue.erase(s->queue.begin() + (long)i);
             return out;
@@ -175,6 +184,7 @@ void worker_main(c2q_server* s)
             s->cv_work.wait(lk, [&] { return s->stop || (!s->queue.empty() && (job = pick(s)) != nullptr); });
             if (!job) break;  // stopping
             s->reserved += job->footprint;
+            s->running_heavy += job->heavy ? 1 : 0;
             ++s->busy;
             job->res.t_admit = s->now();
         }
@@ -187,6 +197,7 @@ void worker_main(c2q_server* s)
             job->res.t_done = s->now();
             job->done       = true;
             s->reserved -= job->footprint;
+            s->running_heavy -= job->heavy ? 1 : 0;
             --s->busy;
             ++s->completed;
         }
@@ -232,6 +243,16 @@ C2Q_EXPORT int c2q_server_create(c2q_server** out, int device, int slots, size_t
     s->loader     = loader;
     for (int i = 0; i < slots; ++i) s->workers.emplace_back(worker_main, s);
     *out = s;
+    return C2Q_OK;
+}
+
+C2Q_EXPORT int c2q_server_set_heavy_limit(c2q_server* s, long long heavy_site_rhs, int max_heavy)
+{
+    if (!s || heavy_site_rhs < 1 || max_heavy < 1) return C2Q_BAD_ARG;
+    std::lock_guard<std::mutex> lk(s->m);
+    s->heavy_site_rhs = heavy_site_rhs;
+    s->max_heavy      = max_heavy;
+    s->cv_work.notify_all();
     return C2Q_OK;
 }
 
@@ -281,6 +302,10 @@ C2Q_EXPORT int c2q_server_submit(c2q_server* s, const c2q_request* req, long lon
         job->res.nsrc    = req->nsrc;
         job->res.t_submit = s->now();
         job->res.footprint_bytes = (long long)job->footprint;
+        {
+            Geom g;
+            job->heavy = make_geom(req->lat, &g) && (long long)g.seo * req->nsrc >= s->heavy_site_rhs;
+        }
         auto it = s->gauges.find(req->gauge_id);
         const bool ok_gauge = it != s->gauges.end() && same_lattice(it->second.g->lat, req->lat);
         const bool fits     = s->gauge_bytes + job->footprint <= s->budget;

@@ -701,6 +701,11 @@ class Server:
         self.h = h
         self._keep = {}
 
+    def set_heavy_limit(self, heavy_site_rhs: int, max_heavy: int):
+        """At most `max_heavy` requests with eo sites x sources >= heavy_site_rhs run
+        at a time (default 2^19 and 1); lighter requests are admitted beside them."""
+        _check(self.lib.c2q_server_set_heavy_limit(self.h, heavy_site_rhs, max_heavy))
+
     def add_gauge(self, gauge_id: int, lattice: Lattice, aos: np.ndarray):
         aos = np.ascontiguousarray(aos, dtype=np.float64).reshape(-1)
         lc = lattice.c()

@@ -514,6 +514,12 @@ C2Q_EXPORT int c2q_server_create(c2q_server** out, int device, int slots, size_t
                                  int rec12);
 C2Q_EXPORT int c2q_server_add_gauge(c2q_server* s, unsigned long long gauge_id, const c2q_lattice* lat,
                                     const double* aos);
+/* A request with eo sites x sources >= heavy_site_rhs fills the GPU by itself;
+ * at most max_heavy such requests run at a time (two side by side share SMs and
+ * L2 and finish later than one after the other), while lighter requests are
+ * admitted beside them.  Default 2^19 site-sources, 1 at a time; max_heavy =
+ * slots lifts the limit. */
+C2Q_EXPORT int c2q_server_set_heavy_limit(c2q_server* s, long long heavy_site_rhs, int max_heavy);
 C2Q_EXPORT int c2q_server_submit(c2q_server* s, const c2q_request* req, long long* ticket);
 /* Blocks until the request has finished (or failed); each ticket is waited on once. */
 C2Q_EXPORT int c2q_server_wait(c2q_server* s, long long ticket, c2q_request_result* out);

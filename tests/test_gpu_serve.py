@@ -108,3 +108,21 @@ def test_request_that_never_fits_fails_with_oom():
     r = server.wait(server.submit(L, 8, 0.15, 0.01, 1, 1))  # unknown gauge id
     assert r["status"] == -5
     server.close()
+
+
+def test_heavy_requests_run_one_at_a_time():
+    """With every request counted as heavy (threshold 1 site-source) and at most
+    one heavy request at a time, three slots run the requests one after another;
+    with the limit lifted they overlap again."""
+    import cl2qcd_b200 as c2q
+    for max_heavy, expect_overlap in ((1, False), (3, True)):
+        server = c2q.host.Server(0, slots=3, precision=16)
+        server.set_heavy_limit(1, max_heavy)
+        lats, _ = _setup(c2q, server)
+        tickets = [server.submit(lats[li], gid, kappa, mu, n, seed) for (li, gid, kappa, mu, n, seed) in REQS]
+        res = [server.wait(t) for t in tickets]
+        server.close()
+        assert all(r["status"] == 0 for r in res), res
+        spans = sorted((r["t_admit"], r["t_done"]) for r in res)
+        overlapped = any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+        assert overlapped == expect_overlap, (max_heavy, spans)
