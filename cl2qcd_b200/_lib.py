@@ -111,6 +111,7 @@ SIGNATURES = {
     "c2q_spinor_eo_convert": (C.c_int, [_P, _P]),
     "c2q_ctx_set_link_format": (C.c_int, [_P, C.c_int]),
     "c2q_ctx_set_autotune": (C.c_int, [_P, C.c_int]),
+    "c2q_ctx_set_sweep_choice": (C.c_int, [_P, C.c_int]),
     "c2q_ctx_tune_report": (C.c_int, [_P, C.c_char_p, C.c_int]),
     "c2q_spinor_eo_destroy": (C.c_int, [_P]),
     "c2q_spinor_eo_upload": (C.c_int, [_P, _D]),

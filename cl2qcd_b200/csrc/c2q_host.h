@@ -60,11 +60,12 @@ struct c2q_ctx {
     // autotuner of the paired-site dslash: launch shape -> chosen configuration
     struct TuneEntry {
         int cfg;
-        float us[4];
+        float us[5];  // per choice; 0 where a choice does not apply to the shape
     };
     std::map<std::vector<int>, TuneEntry> tune;
     c2q::SolverScalars* tune_scratch = nullptr;  // reductions of tuning launches land here
     bool autotune = true;
+    int force_choice = -1;  // >= 0: every paired-site sweep uses this choice where it applies
     int sm_count  = 0;
     // pinned ring of the batched solvers: 4 slots x 16 right-hand sides x 4 doubles
     double* batch_ring = nullptr;

@@ -13,6 +13,7 @@ void pk_dispatch32_c0(const PkParams<32>& prm, int nl, int epi, int dot, int blo
 void pk_dispatch32_c1(const PkParams<32>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
 void pk_dispatch16_c0(const PkParams<16>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
 void pk_dispatch16_c1(const PkParams<16>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
+bool pk2_dispatch(const PkParams<16>& prm, int nl, int epi, int dot, int blocks, cudaStream_t s);
 
 // Resident blocks per SM of a configuration: its launch bound, or what its
 // shared-memory ring leaves room for (228 KB per SM, 1 KB reserved per block).
@@ -79,14 +80,55 @@ static void pk_dispatch(const PkParams<P>& prm, int cfg, int nl, int epi, int do
 // residual update is timed as the same sweep without it), so tuning does not
 // change results.  Shapes first met inside a graph capture use
 // configuration 0 and are not recorded.
-// A tuning choice c selects the kernel configuration c & 1 and the grid
+// A tuning choice c < 4 selects the kernel configuration c & 1 and the grid
 // (c >> 1: grid-stride over resident blocks instead of one block per tile).
-constexpr int PK_CHOICES = 2 * PK_CONFIGS;
+// Choice 4, for FP16 batches of two or more right-hand sides in the temporal
+// gauge (the batched mixed-precision CG), runs two right-hand sides per thread
+// (pdslash2.cuh: each link staged and decoded once for both), an odd last one
+// with configuration 0.
+constexpr int PK_CHOICES    = 2 * PK_CONFIGS;
+constexpr int PK_CHOICE_RB2 = PK_CHOICES;
+
+template <int P>
+static bool pk_rb2_applies(const PkParams<P>& prm)
+{
+    return P == 16 && prm.tg && prm.nrhs >= 2;
+}
+
+// Launch a sweep with a tuning choice.
+template <int P>
+static int pk_run(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int dot, int choice, cudaStream_t s)
+{
+    if constexpr (P == 16) {
+        if (choice == PK_CHOICE_RB2) {
+            const int npair = prm.nrhs / 2;
+            PkParams<16> a  = prm;
+            a.nrhs          = 2 * npair;
+            if (!pk2_dispatch(a, nl, epi, dot, prm.ntiles * npair, s))
+                return fail(ctx, C2Q_BAD_ARG, "no two-sources-per-thread sweep for this shape");
+            if (prm.nrhs & 1) {  // the odd last right-hand side, one per thread
+                PkParams<16> b = prm;
+                b.r[0]         = prm.r[prm.nrhs - 1];
+                b.nrhs         = 1;
+                pk_dispatch<16>(b, 0, nl, epi, dot, pk_grid(ctx, 16, nl, 0, false, b.ntiles, 1), s);
+            }
+            return C2Q_OK;
+        }
+    }
+    const int cfg = choice & 1;
+    pk_dispatch<P>(prm, cfg, nl, epi, dot, pk_grid(ctx, P, nl, cfg, choice >> 1, prm.ntiles, prm.nrhs), s);
+    return C2Q_OK;
+}
 
 template <int P>
 static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int dot, int* cfg)
 {
     *cfg = 0;
+    if (ctx->force_choice >= 0) {  // a fixed choice, where it applies to the shape
+        const int c = ctx->force_choice;
+        *cfg        = (c < PK_CHOICES || (c == PK_CHOICE_RB2 && pk_rb2_applies(prm))) ? c : 0;
+        return C2Q_OK;
+    }
     // the fused CG updates change their residual or solution in place, so their
     // launches are not repeatable: they take the choice timed on the same sweep
     // without the update
@@ -112,14 +154,15 @@ static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int 
         t.r[r].sc     = ctx->tune_scratch + r;
         t.r[r].result = nullptr;
     }
-    c2q_ctx::TuneEntry e{0, {0, 0, 0, 0}};
-    float best = 0;
-    for (int c = 0; c < PK_CHOICES; ++c) {
-        const int blocks = pk_grid(ctx, P, nl, c & 1, c >> 1, t.ntiles, t.nrhs);
-        pk_dispatch<P>(t, c & 1, nl, epi, dot, blocks, ctx->stream);
+    c2q_ctx::TuneEntry e{0, {0, 0, 0, 0, 0}};
+    float best       = 0;
+    const int nchoice = pk_rb2_applies(prm) ? PK_CHOICES + 1 : PK_CHOICES;
+    for (int c = 0; c < nchoice; ++c) {
+        int rc = pk_run<P>(ctx, t, nl, epi, dot, c, ctx->stream);
+        if (rc) return rc;
         C2Q_CUDA(ctx, cudaEventRecord(ctx->ev0, ctx->stream));
-        pk_dispatch<P>(t, c & 1, nl, epi, dot, blocks, ctx->stream);
-        pk_dispatch<P>(t, c & 1, nl, epi, dot, blocks, ctx->stream);
+        pk_run<P>(ctx, t, nl, epi, dot, c, ctx->stream);
+        pk_run<P>(ctx, t, nl, epi, dot, c, ctx->stream);
         C2Q_CUDA(ctx, cudaEventRecord(ctx->ev1, ctx->stream));
         C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ev1));
         C2Q_CUDA(ctx, cudaGetLastError());
@@ -130,7 +173,7 @@ static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int 
             best  = e.us[c];
             e.cfg = c;
         }
-        ctx->launches += 3;
+        ctx->launches += 3 * ((c == PK_CHOICE_RB2 && (t.nrhs & 1)) ? 2 : 1);
     }
     ctx->tune[key] = e;
     *cfg           = e.cfg;
@@ -208,8 +251,6 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     int choice       = 0;
     int rc           = pk_choose<P>(ctx, prm, nl, B.epi, B.dot_mode, &choice);
     if (rc) return rc;
-    const int cfg    = choice & 1;
-    const int blocks = pk_grid(ctx, P, nl, cfg, choice >> 1, prm.ntiles, B.n);
     c2q_ctx::Timed tm{};
     if (ctx->profiling) {
         tm.a     = profile_event(ctx);
@@ -231,12 +272,13 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
         tm.bytes           = (double)ref->geom.seo * (links * lk + B.n * per_rhs);
         cudaEventRecord(tm.a, ctx->stream);
     }
-    pk_dispatch<P>(prm, cfg, nl, B.epi, B.dot_mode, blocks, ctx->stream);
+    rc = pk_run<P>(ctx, prm, nl, B.epi, B.dot_mode, choice, ctx->stream);
+    if (rc) return rc;
     if (ctx->profiling) {
         cudaEventRecord(tm.b, ctx->stream);
         ctx->timed.push_back(tm);
     }
-    ctx->launches++;
+    ctx->launches += choice == PK_CHOICE_RB2 && (B.n & 1) ? 2 : 1;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
 }
@@ -391,6 +433,13 @@ C2Q_EXPORT int c2q_ctx_set_autotune(c2q_ctx* ctx, int enable)
     return C2Q_OK;
 }
 
+C2Q_EXPORT int c2q_ctx_set_sweep_choice(c2q_ctx* ctx, int choice)
+{
+    if (!ctx || choice < -1 || choice > PK_CHOICE_RB2) return C2Q_BAD_ARG;
+    ctx->force_choice = choice;
+    return C2Q_OK;
+}
+
 C2Q_EXPORT int c2q_ctx_tune_report(const c2q_ctx* ctx, char* buf, int len)
 {
     if (!ctx) return C2Q_BAD_ARG;
@@ -399,11 +448,15 @@ C2Q_EXPORT int c2q_ctx_tune_report(const c2q_ctx* ctx, char* buf, int len)
     for (const auto& kv : ctx->tune) {
         const std::vector<int>& k = kv.first;
         snprintf(line, sizeof line,
-                 "prec=%d links=%d epi=%d dot=%d phases=%d nrhs=%d sites=%d choice=%d (config %d, %s grid) "
-                 "us=[%.1f, %.1f, %.1f, %.1f]\n",
-                 k[0], k[1] == 6 ? 12 : 18, k[2], k[3], k[4], k[5], k[6], kv.second.cfg, kv.second.cfg & 1,
-                 (kv.second.cfg >> 1) ? "grid-stride" : "per-tile", kv.second.us[0], kv.second.us[1], kv.second.us[2],
-                 kv.second.us[3]);
+                 "prec=%d links=%d epi=%d dot=%d phases=%d nrhs=%d sites=%d choice=%d (%s) "
+                 "us=[%.1f, %.1f, %.1f, %.1f, %.1f]\n",
+                 k[0], k[1] == 6 ? 12 : 18, k[2], k[3], k[4], k[5], k[6], kv.second.cfg,
+                 kv.second.cfg == PK_CHOICE_RB2 ? "two right-hand sides per thread"
+                 : (kv.second.cfg >> 1)         ? ((kv.second.cfg & 1) ? "config 1, grid-stride grid"
+                                                                       : "config 0, grid-stride grid")
+                                                : ((kv.second.cfg & 1) ? "config 1, per-tile grid"
+                                                                       : "config 0, per-tile grid"),
+                 kv.second.us[0], kv.second.us[1], kv.second.us[2], kv.second.us[3], kv.second.us[4]);
         out += line;
     }
     if (buf && len > 0) {

@@ -348,18 +348,17 @@ __device__ __forceinline__ void staged_operand(const uint4* st, C2 q[12], float2
     }
 }
 
-// One hop from a stage: the neighbour slot (and, for a backward hop, its
-// link) may hold the two sites swapped -- SWP, set for the time hops across
-// the fold.  A forward hop's link sits at the output slot and is never swapped.
-// w: the hop weight of each lane (the two sites) and its negations.
-template <int P, int NL, int MU, bool BACK, bool SWP, bool KREAL>
-__device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, const Kc& w)
+// The spinor half of one hop: the decoded link u applied to the staged
+// neighbour spinor st (projection, SU(3) products, accumulation).  The
+// neighbour slot may hold the two sites swapped -- SWP, set for the time hops
+// across the fold.  w: the hop weight of each lane (the two sites) and its
+// negations.
+template <int P, int MU, bool BACK, bool SWP, bool KREAL>
+__device__ __forceinline__ void pk_hop_spinor(C2 acc[12], const uint4* st, const C2 u[9], const Kc& w)
 {
     using T          = Proj<MU>;
     constexpr int c0 = BACK ? NegUnit<T::c0>::value : T::c0;
     constexpr int c1 = BACK ? NegUnit<T::c1>::value : T::c1;
-    C2 u[9];
-    staged_link<P, NL, BACK && SWP>(st + PkChunks<P, NL>::SPC * PK_THREADS, u);
     Kc k;
     C2 h[3];
     if constexpr (P == 16) {
@@ -389,6 +388,17 @@ __device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, const Kc& w)
         for (int col = 0; col < 3; ++col) h[col] = proj_vals<c1>(psi[3 + col], psi[3 * T::p1 + col]);
         pk_channel<1, T::p1, c1, BACK, KREAL>(acc, h, u, k);
     }
+}
+
+// One hop from a stage: its link (staged after the spinor) decoded, then the
+// spinor half.  A forward hop's link sits at the output slot and is never
+// swapped; a backward hop's link swaps with its neighbour slot.
+template <int P, int NL, int MU, bool BACK, bool SWP, bool KREAL>
+__device__ __forceinline__ void pk_hop(C2 acc[12], const uint4* st, const Kc& w)
+{
+    C2 u[9];
+    staged_link<P, NL, BACK && SWP>(st + PkChunks<P, NL>::SPC * PK_THREADS, u);
+    pk_hop_spinor<P, MU, BACK, SWP, KREAL>(acc, st, u, w);
 }
 
 // A half-spinor channel through an identity link: acc_A += k h, acc_PP += conj(c) k h.

@@ -92,6 +92,10 @@ class System:
         """Links read by the explicit operator calls: 18-real (default) or 12-real."""
         _check(self.lib.c2q_ctx_set_link_format(self.h, int(bool(rec12))), self.h, self.lib)
 
+    def set_sweep_choice(self, choice: int):
+        """Pin the launch choice of the reduced-precision sweeps (-1: the autotuner's)."""
+        _check(self.lib.c2q_ctx_set_sweep_choice(self.h, choice), self.h, self.lib)
+
     def tune_report(self) -> str:
         """The launch configurations the autotuner chose, one line per launch shape."""
         n = self.lib.c2q_ctx_tune_report(self.h, None, 0)

@@ -286,6 +286,13 @@ C2Q_EXPORT int c2q_ctx_set_link_format(c2q_ctx* ctx, int rec12);
  * shape into buf (NUL-terminated, truncated to len) and returns the length
  * needed including the NUL. */
 C2Q_EXPORT int c2q_ctx_set_autotune(c2q_ctx* ctx, int enable);
+/* (no counterpart in the reference) Pins the launch choice of every
+ * reduced-precision sweep on the context instead of the autotuner's: 0..3 =
+ * launch configuration (choice & 1) with one block per tile (choice >> 1 = 0)
+ * or a grid-stride grid (1); 4 = two right-hand sides per thread, for FP16
+ * batches of two or more in the temporal gauge (elsewhere choice 0); -1 = the
+ * autotuner decides (default).  Every choice gives bitwise the same results. */
+C2Q_EXPORT int c2q_ctx_set_sweep_choice(c2q_ctx* ctx, int choice);
 C2Q_EXPORT int c2q_ctx_tune_report(const c2q_ctx* ctx, char* buf, int len);
 /* convert_to_eoprec / convert_from_eoprec (physics/lattices/spinorfield_eo.cpp:372-410):
  * `full` is a host spinor[V]; `even` gets the sites with x+y+z+t even (FP64 fields). */

@@ -148,3 +148,55 @@ def test_zero_source_in_batch(port, system, O, precision):
     assert not np.any(x0.dump())
     with pytest.raises(c2q.SolverStuck):
         c2q.host.cg(x0, A, gf, bs[1], c2q.SolverParameters(solver="cg", prec=1e-22, cgmax=50), add)
+
+
+@pytest.mark.parametrize("rec12", [True, False])
+@pytest.mark.parametrize("nsrc", [2, 5, 12])
+def test_two_sources_per_thread_is_bitwise_the_same(port, system, O, nsrc, rec12):
+    """The FP16 batched sweeps that run two right-hand sides per thread (each link
+    staged and decoded once for both; sweep choice 4) give bitwise the solutions
+    of the one-source-per-thread sweeps (choice 0), an odd last source included,
+    and every solution meets the true-residual bar of the oracle's operator."""
+    import cl2qcd_b200 as c2q
+    L, g, gf = _problem(port, c2q, system, 8, 8, 0.3, 5)
+    kappa, mubar = 0.155, 2 * 0.155 * 0.008
+    add = c2q.AdditionalParameters(kappa, mubar)
+    A = c2q.host.QplusQminus_eo()
+    srcs = [c2q.host.generate_source(L.seo, "gaussian", 300 + k) for k in range(nsrc)]
+    bs = [c2q.Spinorfield_eo(system, L, s) for s in srcs]
+    P = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=1e-10, cgmax=5000, precision=16, use_rec12=rec12)
+    out = {}
+    try:
+        for choice in (0, 4):
+            system.set_sweep_choice(choice)
+            xs = [c2q.Spinorfield_eo(system, L) for _ in srcs]
+            reps = []
+            c2q.host.cg_multi(xs, A, gf, bs, P, add, reps)
+            out[choice] = ([x.dump() for x in xs], [r["iterations"] for r in reps])
+    finally:
+        system.set_sweep_choice(-1)
+    assert out[0][1] == out[4][1]
+    for k in range(nsrc):
+        assert np.array_equal(out[0][0][k], out[4][0][k]), k
+        r = port.apply(O.OP_QPQM_EO, out[4][0][k], g, kappa, mubar)
+        assert np.linalg.norm(r - srcs[k]) / np.linalg.norm(srcs[k]) <= 1.5e-10
+
+
+def test_sweep_choice_falls_back_where_it_does_not_apply(port, system, O):
+    """Choice 4 on an FP32 batch (no two-per-thread kernel) runs choice 0."""
+    import cl2qcd_b200 as c2q
+    L, g, gf = _problem(port, c2q, system, 8, 8, 0.3, 5)
+    add = c2q.AdditionalParameters(0.15, 0.003)
+    srcs = [c2q.host.generate_source(L.seo, "z2", 400 + k) for k in range(3)]
+    bs = [c2q.Spinorfield_eo(system, L, s) for s in srcs]
+    P = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=1e-10, cgmax=5000, precision=32, use_rec12=True)
+    res = {}
+    try:
+        for choice in (0, 4):
+            system.set_sweep_choice(choice)
+            xs = [c2q.Spinorfield_eo(system, L) for _ in srcs]
+            c2q.host.cg_multi(xs, c2q.host.QplusQminus_eo(), gf, bs, P, add)
+            res[choice] = [x.dump() for x in xs]
+    finally:
+        system.set_sweep_choice(-1)
+    assert all(np.array_equal(a, b) for a, b in zip(res[0], res[4]))
