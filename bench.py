@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", type=int, default=16, choices=[16, 32, 64])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-large", action="store_true", help="skip the 64^3x128 (config 5) section of the default run")
     ap.add_argument("--serve", action="store_true",
                     help="serving sweep only: Poisson requests at rising rates, p50/p99 latency and solves/s")
     ap.add_argument("--serve-requests", type=int, default=16)
@@ -329,18 +330,22 @@ def dslash_gbs(c2q, system, lat, gf, b, e0, e1, n=20):
     return out
 
 
-def large_volume(c2q, system, e0, e1):
+def large_volume(c2q, system, e0, e1, bicgstab_cgmax=2000, oracle_check_solution=False):
     """64^3x128 (16.8 M eo sites), eps 0.2, kappa 0.1625, mu 0.003, one Gaussian
     source: dslash GB/s per precision (FP64 gauge 18-real vs 12-real) and the
-    solve time to a true residual 1e-10 of FP64 CG, FP64 BiCGStab (on Aee) and
-    mixed-precision CG (FP16 / FP32 inner); each CG timed on its second solve."""
+    solve time to a true residual 1e-10 of FP64 CG, FP64 BiCGStab (on Aee; it does
+    not converge on this operator, nor does the reference's, so it is bounded by
+    bicgstab_cgmax) and mixed-precision CG (FP16 / FP32 inner); each CG timed on its
+    second solve.  With oracle_check_solution the mixed FP16 solution's true
+    residual is recomputed by the oracle (the reference's kernels on the host)."""
     import torch
     ns, nt, kappa, mu = 64, 128, 0.1625, 0.003
     lat = c2q.Lattice(ns, nt, 1.0, 0.0)
     t = time.time()
     g = c2q.host.generate_gaugefield(lat, 0.2, 64128)
     gf = c2q.Gaugefield(system, lat, g)
-    del g
+    if not oracle_check_solution:
+        del g
     b = c2q.host.generate_source(lat.seo, "gaussian", 128)
     setup_s = time.time() - t
     out = {"lattice": "64^3x128", "eo_sites": lat.seo, "kappa": kappa, "mu": mu, "eps": 0.2,
@@ -354,7 +359,8 @@ def large_volume(c2q, system, e0, e1):
                     c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=64)),
         # the reference's BiCGStab "save" variant (true-residual recheck), bounded
         "fp64_bicgstab_save": (c2q.host.bicgstab, c2q.host.Aee(),
-                               c2q.SolverParameters(solver="bicgstab_save", prec=REL_TOL ** 2 * b2, cgmax=2000)),
+                               c2q.SolverParameters(solver="bicgstab_save", prec=REL_TOL ** 2 * b2,
+                                                    cgmax=bicgstab_cgmax)),
         "mixed_fp16_cg": (c2q.host.cg, c2q.host.QplusQminus_eo(),
                           c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=REL_TOL, cgmax=40000, precision=16,
                                                use_rec12=True, use_graph=True)),
@@ -392,6 +398,18 @@ def large_volume(c2q, system, e0, e1):
     ref = sols["fp64_cg"]
     for name in ("mixed_fp16_cg", "mixed_fp32_cg"):
         out[name]["rel_err_vs_fp64_cg"] = float(np.linalg.norm(sols[name] - ref) / np.linalg.norm(ref))
+    out["speedup_mixed_fp16_vs_fp64_cg"] = out["fp64_cg"]["seconds"] / out["mixed_fp16_cg"]["seconds"]
+    if oracle_check_solution:
+        import oracle as O
+        kind = "reference" if O.available("reference") else "port"
+        o = O.Oracle(kind)
+        o.set_lattice(ns, nt, 1.0, 0.0)
+        r = o.apply(O.OP_QPQM_EO, sols["mixed_fp16_cg"], g, kappa, 2 * kappa * mu)
+        r -= b
+        rel = float(np.linalg.norm(r) / np.sqrt(b2))
+        out["oracle_check"] = {"solution": "mixed_fp16_cg", "true_resid_rel": rel, "pass": rel <= REL_TOL * (1 + 1e-6),
+                               "oracle": kind, "operator": "QplusQminus_eo on the 18-real FP64 links as generated"}
+        del g, r
     return out
 
 
@@ -870,6 +888,14 @@ def main():
     config1 = config1_gpu(c2q, system, e0, e1)
     # serving stream at one arrival rate (the full sweep: --serve)
     serving = serving_run(c2q, [1.0], args.serve_requests) if rank == 0 and ws == 1 else None
+    # config 5, 64^3x128 (BiCGStab bounded at 300 iterations: it does not converge there)
+    large = None
+    if rank == 0 and ws == 1 and not args.no_large:
+        try:
+            large = large_volume(c2q, system, e0, e1, bicgstab_cgmax=300,
+                                 oracle_check_solution=not args.no_cpu_baseline)
+        except Exception as e:  # reported, not fatal
+            large = {"error": repr(e)}
 
     cpu_baseline = None
     rec_iters, _rec = recorded_fp64_iterations()
@@ -930,6 +956,7 @@ def main():
             "multi_rhs": mrhs,
             "config1": config1,
             "serving": serving,
+            "large_volume": large,
             "autotune": system.tune_report().strip().splitlines(),
         }
         print(json.dumps(line))
