@@ -173,8 +173,10 @@ C2Q_EXPORT int c2q_params_from_kv(const char* text, c2q_params* p)
     if (!text || !p) return bad("c2q_params_from_kv: null argument");
     static const std::map<std::string, int> solvers = {
         {"cg", C2Q_SOLVER_CG}, {"bicgstab", C2Q_SOLVER_BICGSTAB}, {"bicgstab_save", C2Q_SOLVER_BICGSTAB_SAVE}};
+    // common::action (common_header_files/types.hpp:198): the fermion matrices
+    // here take wilson and twistedmass; the others parse, and the calls reject them
     static const std::map<std::string, int> actions = {
-        {"wilson", C2Q_ACTION_WILSON}, {"twistedmass", C2Q_ACTION_TWISTEDMASS}, {"clover", -1}, {"rooted_stagg", -2}};
+        {"wilson", C2Q_ACTION_WILSON}, {"clover", 2}, {"twistedmass", C2Q_ACTION_TWISTEDMASS}, {"rooted_stagg", 7}};
     static const std::map<std::string, int> starts = {
         {"cold_start", C2Q_START_COLD}, {"cold", C2Q_START_COLD}, {"hot_start", C2Q_START_HOT},
         {"hot", C2Q_START_HOT}, {"start_from_source", C2Q_START_CONTINUE}, {"source", C2Q_START_CONTINUE},
@@ -227,11 +229,8 @@ C2Q_EXPORT int c2q_params_from_kv(const char* text, c2q_params* p)
             if (val.size() >= sizeof q.initial_conf) return bad(where + "initialConf path too long");
             strcpy(q.initial_conf, val.c_str());
         } else if (key == "ignoreChecksumErrors") rc = need(to_bool(val, &q.ignore_checksum_errors));
-        else if (key == "fermionAction") {
-            rc = need(to_enum(val, actions, &iv));
-            if (!rc && iv < 0) return bad(where + "fermionAction '" + val + "' lies outside this library (wilson, twistedmass)");
-            if (!rc) q.fermion_action = iv;
-        } else if (key == "kappa") rc = need(to_double(val, &q.kappa));
+        else if (key == "fermionAction") rc = need(to_enum(val, actions, &q.fermion_action));
+        else if (key == "kappa") rc = need(to_double(val, &q.kappa));
         else if (key == "mu") rc = need(to_double(val, &q.mu));
         else if (key == "thetaFermionSpatial") rc = need(to_double(val, &q.lat.theta_s));
         else if (key == "thetaFermionTemporal") rc = need(to_double(val, &q.lat.theta_t));
@@ -268,13 +267,12 @@ C2Q_EXPORT int c2q_params_from_kv(const char* text, c2q_params* p)
     // checks of this path (the reference checks these when it builds the lattice and the kernels)
     if (q.lat.ns < 2 || q.lat.nt < 2 || (q.lat.ns & 1) || (q.lat.nt & 1))
         return bad("nSpace and nTime must be even and at least 2");
-    if (q.precision != 64) return bad("precision must be 64 (the reference computes in FP64 only)");
+    if (q.precision != 64 && q.precision != 32) return bad("precision must be 64 or 32 (bits)");
     if (q.solver.precision != 64 && q.solver.precision != 32 && q.solver.precision != 16)
         return bad("b200.innerPrecision must be 64, 32 or 16");
     if (q.solver.cgmax < 0 || q.solver.iter_refresh <= 0 || q.solver.resid_check_every <= 0)
         return bad("solverMaxIterations must be >= 0, solverRestartEvery and solverResiduumCheckEvery > 0");
-    if (q.correlator_direction != 0 && q.correlator_direction != 3)
-        return bad("correlatorDirection must be 0 or 3");
+    if (q.correlator_direction < 0 || q.correlator_direction > 3) return bad("correlatorDirection must be 0..3");
     if (q.n_sources < 0) return bad("nSources must be >= 0");
     q.mubar = 2.0 * q.kappa * q.mu;
     *p      = q;

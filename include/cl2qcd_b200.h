@@ -167,11 +167,13 @@ typedef struct {
 #define C2Q_CONTENT_Z2 3
 typedef struct {
     c2q_lattice lat;              /* nSpace, nTime, thetaFermion*, chemical potential */
-    int fermion_action;           /* fermionAction: C2Q_ACTION_WILSON or C2Q_ACTION_TWISTEDMASS */
+    int fermion_action;           /* fermionAction as common::action: C2Q_ACTION_WILSON (1), clover (2),
+                                     C2Q_ACTION_TWISTEDMASS (3), rooted_stagg (7); the fermion
+                                     matrices here take the wilson and twisted-mass actions */
     double kappa, mu;             /* kappa, mu */
     double mubar;                 /* 2 kappa mu */
     int use_eo;                   /* useEO */
-    int precision;                /* precision (64) */
+    int precision;                /* precision in bits (64 or 32; this library's FP64 path needs 64) */
     int use_merge_kernels_fermion, use_merge_kernels_spinor;
     c2q_solver_params solver;     /* solver keys; use_rec12 = useReconstruct12; [b200] keys */
     int start_condition;          /* C2Q_START_* */
@@ -180,7 +182,7 @@ typedef struct {
     int source_type, source_content, n_sources;
     int source_pos[4];            /* sourceX, sourceY, sourceZ, sourceT */
     int measure_correlators;      /* measureCorrelators */
-    int correlator_direction;     /* correlatorDirection (0 or 3) */
+    int correlator_direction;     /* correlatorDirection (0 = t .. 3 = z; c2q_correlator_ps takes 0 and 3) */
 } c2q_params;
 /* The reference's defaults (the constructors of meta/parameters*.cpp). */
 C2Q_EXPORT void c2q_params_default(c2q_params* p);

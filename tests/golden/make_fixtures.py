@@ -305,6 +305,31 @@ def extract_blas_kats(ref: str) -> dict:
     return out
 
 
+def extract_params_kats(ref: str) -> dict:
+    """meta/inputparameters_test.cpp: the values its checkDefaults (empty input file,
+    the double-precision branch), input_file2 (meta/test_input_2) and aliases
+    (meta/test_input_aliases) cases require, with the input files' text verbatim."""
+    src = open(os.path.join(ref, "meta/inputparameters_test.cpp")).read()
+    blocks = {"defaults": src[src.index("void checkDefaults"):src.index("BOOST_AUTO_TEST_CASE(defaults)")],
+              "input_file2": src[src.index("BOOST_AUTO_TEST_CASE(input_file2)"):
+                                 src.index("BOOST_AUTO_TEST_CASE(command_line1)")],
+              "aliases": src[src.index("BOOST_AUTO_TEST_CASE(aliases)"):src.index("BOOST_AUTO_TEST_CASE(help)")]}
+    files = {"defaults": "test_input_1", "input_file2": "test_input_2", "aliases": "test_input_aliases"}
+    out = {"where": "meta/inputparameters_test.cpp"}
+    for name, body in blocks.items():
+        body = body.split("#else")[0] + (body.split("#endif")[1] if "#endif" in body else "")
+        expect = {}
+        for getter, val in re.findall(r"BOOST_REQUIRE_EQUAL\(params\.(get_\w+|is_\w+)\(\)(?:\.size\(\))?,\s*([^;]+)\);",
+                                      body):
+            v = val.strip()[:-1].strip() if val.strip().endswith(")") else val.strip()
+            if getter in expect:
+                continue
+            expect[getter] = v
+        out[name] = {"input_file": f"meta/{files[name]}",
+                     "input_text": open(os.path.join(ref, "meta", files[name])).read(), "expect": expect}
+    return out
+
+
 def make_ref_outputs(path):
     import oracle as O
     R = O.Oracle("reference")
@@ -343,6 +368,7 @@ if __name__ == "__main__":
         raise SystemExit("name the reference tree: make_fixtures.py /path/to/reference, or set CL2QCD_REFERENCE")
     kats = extract_kats(ref)
     kats["blas_and_merged_eo"] = extract_blas_kats(ref)
+    kats["inputparameters"] = extract_params_kats(ref)
     kats["ildg_conf00200"] = decode_conf00200(ref)
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
         json.dump(kats, f, indent=1, sort_keys=True)

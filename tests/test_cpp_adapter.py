@@ -77,10 +77,10 @@ def test_parser_rules(lib):
     # a second text overrides the first
     assert lib.c2q_params_from_kv(b"kappa=0.16\nmu=0.005", C.byref(P)) == 0
     assert P.mubar == pytest.approx(0.0016) and P.lat.ns == 8
-    for bad, why in ((b"nSpace=7", b"even"), (b"kappa=abc", b"invalid value"), (b"fermionAction=clover", b"outside"),
+    for bad, why in ((b"nSpace=7", b"even"), (b"kappa=abc", b"invalid value"), (b"fermionAction=foo", b"invalid value"),
                      (b"noSuchKey=1", b"unknown option"), (b"mu=1\nmu=2", b"more than once"),
-                     (b"precision=32", b"precision"), (b"justtext", b"name = value"),
-                     (b"[b200]\ninnerPrecision=8", b"innerPrecision")):
+                     (b"precision=16", b"precision"), (b"justtext", b"name = value"),
+                     (b"[b200]\ninnerPrecision=8", b"innerPrecision"), (b"startCondition=foo", b"invalid value")):
         before = bytes(P)
         assert lib.c2q_params_from_kv(bad, C.byref(P)) == L.BAD_ARG, bad
         assert why in lib.c2q_params_last_error(), (bad, lib.c2q_params_last_error())
