@@ -56,6 +56,7 @@ struct BlasArgs {
 template <int P>
 __global__ void __launch_bounds__(BLAS_THREADS) blas_kernel(const BlasArgs<P> A)
 {
+    if (halted(A.red)) return;  // a stopped device-driven solve: every block leaves
     using R      = typename Prec<P>::R;
     const int i  = blockIdx.x * blockDim.x + threadIdx.x;
     double dv[4] = {0.0, 0.0, 0.0, 0.0};

@@ -66,6 +66,9 @@ struct c2q_ctx {
     c2q::SolverScalars* tune_scratch = nullptr;  // reductions of tuning launches land here
     bool autotune = true;
     int force_choice = -1;  // >= 0: every paired-site sweep uses this choice where it applies
+    // launch predicate of a device-driven solve (SolverScalars::halt): while set,
+    // every reducing BLAS and dslash launch skips its work once *halt_dev != 0
+    const int* halt_dev = nullptr;
     int sm_count  = 0;
     // pinned ring of the batched solvers: 4 slots x 16 right-hand sides x 4 doubles
     double* batch_ring = nullptr;
@@ -203,6 +206,7 @@ struct BlasSpec {
     const c2q_spinor_eo *x = nullptr, *y = nullptr, *z = nullptr;
     int dot = 0;
     int fin = FIN_STORE_RESULT;
+    int fin_arg = 0;
 };
 int launch_blas(c2q_ctx* ctx, const BlasSpec& s);
 int launch_cg_update(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* r, const c2q_spinor_eo* p,

@@ -182,6 +182,7 @@ __device__ __forceinline__ void do_direction(Cplx<typename Prec<P>::R> acc[12], 
 template <int P, int NL, int EPI, int DOT, int PH>
 __global__ void __launch_bounds__(128) dslash_kernel(const DslashParams<P> prm)
 {
+    if (halted(prm.red)) return;  // a stopped device-driven solve: every block leaves
     using R       = typename Prec<P>::R;
     const Geom& g = prm.g;
     const int i   = blockIdx.x * blockDim.x + threadIdx.x;

@@ -227,6 +227,7 @@ static RedArgs red_args(c2q_ctx* ctx, int fin)
     r.result   = ctx->red_result;
     r.sc       = ctx->scalars;
     r.fin      = fin;
+    r.halt     = ctx->halt_dev;
     return r;
 }
 
@@ -546,7 +547,8 @@ static int blas_typed(c2q_ctx* ctx, const BlasSpec& s, const c2q_spinor_eo* ref)
         int rc = ensure_partials(ctx, s.dot == 3 ? 2 * (size_t)blocks : (size_t)blocks);
         if (rc) return rc;
     }
-    A.red = red_args(ctx, s.fin);
+    A.red         = red_args(ctx, s.fin);
+    A.red.fin_arg = s.fin_arg;
     blas_kernel<P><<<blocks, BLAS_THREADS, 0, ctx->stream>>>(A);
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());

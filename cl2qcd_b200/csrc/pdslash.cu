@@ -150,6 +150,7 @@ static int pk_choose(c2q_ctx* ctx, const PkParams<P>& prm, int nl, int epi, int 
     PkParams<P> t = prm;
     t.red.sc      = ctx->tune_scratch + PK_MAX_RHS;
     t.red.result  = ctx->tune_scratch[PK_MAX_RHS].aux;
+    t.red.halt    = nullptr;  // timing launches always run
     for (int r = 0; r < t.nrhs; ++r) {
         t.r[r].sc     = ctx->tune_scratch + r;
         t.r[r].result = nullptr;
@@ -246,6 +247,7 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
     prm.red.result   = ctx->red_result;
     prm.red.sc       = ctx->scalars;
     prm.red.fin      = B.fin;
+    prm.red.halt     = ctx->halt_dev;
     const bool r12   = gkind_is_r12(gkind);  // else 18-real
     const int nl     = r12 ? 6 : 9;
     int choice       = 0;

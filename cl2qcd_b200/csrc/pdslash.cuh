@@ -501,6 +501,7 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
     static_assert(S::STAGES == 2 || S::STAGES == 3, "the prologue below issues one or two stages");
     static_assert(DOT != DOT_XUPD || EPI != EPI_AXPY, "the solution update shares the EPI_AXPY operand slot");
     constexpr bool RED = DOT != DOT_NONE && DOT != DOT_XUPD;  // a reduction is fused
+    if (halted(prm.red)) return;  // a stopped device-driven solve: every block leaves
     extern __shared__ uint4 ring[];
     uint4* mine     = ring + threadIdx.x;
     const PkGeom& g = prm.g;

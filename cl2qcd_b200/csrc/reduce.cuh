@@ -54,6 +54,19 @@ struct SolverScalars {
     double resid;        // last |r|^2 written by a reducing kernel
     double aux[2];       // extra reduction slot (BiCGStab (t,t), true residual, ...)
     int flag;            // nonzero: a division by zero / NaN was seen
+    int halt;            // BiCGStab: nonzero stops every later predicated launch (HALT_*)
+    int halt_next;       // BiCGStab: the next iteration's opening test, moved into halt at its start
+    int pad_;
+    double thr;          // BiCGStab: stopping threshold on |r|^2
+};
+
+// Why a device-driven BiCGStab stopped (SolverScalars::halt bits).
+enum HaltBits : int {
+    HALT_STUCK     = 1,   // (rhat, r_new) vanished: SolverStuck in this iteration
+    HALT_NAN       = 2,   // |r|^2 is NaN at this iteration's test
+    HALT_CONV      = 4,   // |r|^2 < thr at this iteration's test
+    HALT_NAN_NEXT  = 8,   // the same two tests, due at the top of the next iteration
+    HALT_CONV_NEXT = 16,
 };
 
 // What the last block does with the reduced value(s).
@@ -62,6 +75,15 @@ enum Finisher : int {
     FIN_CG_ALPHA     = 1,  // rho = sum; alpha = omega / rho
     FIN_CG_BETA      = 2,  // rho_next = (sum,0); resid = sum; beta = rho_next/omega; omega = rho_next
     FIN_CG_OMEGA     = 3,  // omega = (sum,0) ; resid = sum  (refresh iteration, (r,r))
+    // BiCGStab, physics/algorithms/solvers/bicgstab.cpp:566-733 (fast) and :401-564 (save)
+    FIN_BI_REFRESH = 4,  // <rhat,rn>, <rhat,rhat>: rho; resid; the iteration's opening test
+    FIN_BI_ALPHA   = 5,  // tmp1 = (rhat, v); alpha = rho / tmp1
+    FIN_BI_OMEGA   = 6,  // <t,s>, <t,t>: tmp1, tmp2; omega = tmp1 / tmp2
+    FIN_BI_RESID   = 7,  // resid = |rn|^2 (fin_arg: apply the stopping test now -- save)
+    FIN_BI_BETA    = 8,  // fast: rho_next = (rhat, rn), stuck test, beta, tmp2 = -beta omega, rho;
+                         // fin_arg: the next iteration's opening test (it is no refresh)
+    FIN_BIS_INIT   = 9,  // save refresh: alpha = omega = rho = 1
+    FIN_BIS_RHO    = 10, // save: rho_next = (rhat, rn), stuck test, beta, tmp2 = -beta omega, rho
 };
 
 struct RedArgs {
@@ -70,7 +92,56 @@ struct RedArgs {
     double* result;        // FIN_STORE_RESULT destination (NV doubles)
     SolverScalars* sc;     // solver scalars for the CG finishers
     int fin;
+    int fin_arg = 0;       // finisher option (FIN_BI_RESID, FIN_BI_BETA)
+    // Launch predicate: when set and *halt is nonzero every block returns at
+    // once (a stopped device-driven solve; nothing is read or written).
+    const int* halt = nullptr;
 };
+
+__device__ __forceinline__ bool halted(const RedArgs& ra) { return ra.halt && *(volatile const int*)ra.halt; }
+
+// Complex arithmetic of the BiCGStab finishers, rounded operation by operation
+// (no contraction into FMAs) as the host's complexdivide / complexmult
+// (common_header_files/operations_complex.hpp:35-66) round them.
+__device__ __forceinline__ void cx_div(double* out, const double* n, const double* d, int* flag)
+{
+    const double norm = __dadd_rn(__dmul_rn(d[0], d[0]), __dmul_rn(d[1], d[1]));
+    if (!(norm > 0.0)) *flag = 1;
+    const double re = __dadd_rn(__dmul_rn(n[0], d[0]), __dmul_rn(n[1], d[1]));
+    const double im = __dsub_rn(__dmul_rn(n[1], d[0]), __dmul_rn(n[0], d[1]));
+    out[0]          = __ddiv_rn(re, norm);
+    out[1]          = __ddiv_rn(im, norm);
+}
+__device__ __forceinline__ void cx_mul(double* out, const double* a, const double* b)
+{
+    const double re = __dsub_rn(__dmul_rn(a[0], b[0]), __dmul_rn(a[1], b[1]));
+    const double im = __dadd_rn(__dmul_rn(a[1], b[0]), __dmul_rn(a[0], b[1]));
+    out[0]          = re;
+    out[1]          = im;
+}
+// beta = (rho_next / rho)(alpha / omega), tmp1 = beta omega, tmp2 = -tmp1, rho = rho_next
+// (bicgstab.cpp:712-720 fast, :473-479 save)
+__device__ __forceinline__ void bicg_beta(SolverScalars* s)
+{
+    const double mone[2] = {-1.0, 0.0};
+    cx_div(s->tmp1, s->rho_next, s->rho, &s->flag);
+    cx_div(s->tmp2, s->alpha, s->omega, &s->flag);
+    cx_mul(s->beta, s->tmp1, s->tmp2);
+    cx_mul(s->tmp1, s->beta, s->omega);
+    cx_mul(s->tmp2, mone, s->tmp1);
+    s->rho[0] = s->rho_next[0];
+    s->rho[1] = s->rho_next[1];
+}
+__device__ __forceinline__ bool bicg_stuck(const double* r)
+{
+    return fabs(r[0]) < 1e-25 && fabs(r[1]) < 1e-25;  // bicgstab.cpp:467, :705
+}
+// the stopping test on |r|^2 (NaN -> SolverStuck, below thr -> converged)
+__device__ __forceinline__ int bicg_test(const SolverScalars* s, int nan_bit, int conv_bit)
+{
+    if (s->resid != s->resid) return nan_bit;
+    return s->resid < s->thr ? conv_bit : 0;
+}
 
 __device__ __forceinline__ void cdiv_store(double* out, const double* n, const double* d, int* flag)
 {
@@ -161,6 +232,58 @@ __device__ __forceinline__ void finish_group(const RedArgs& ra, double* smem, in
                 s->omega[0] = acc[0];
                 s->omega[1] = 0.0;
                 s->resid    = acc[0];
+                break;
+            }
+            case FIN_BI_REFRESH: {  // NV = 4: <rhat, rn>, <rhat, rhat> with rhat = rn
+                s->rho[0] = acc[0];
+                s->rho[1] = acc[NV > 1 ? 1 : 0];
+                s->resid  = acc[NV > 2 ? 2 : 0];
+                s->halt |= bicg_test(s, HALT_NAN, HALT_CONV);
+                break;
+            }
+            case FIN_BI_ALPHA: {
+                s->tmp1[0] = acc[0];
+                s->tmp1[1] = acc[NV > 1 ? 1 : 0];
+                cx_div(s->alpha, s->rho, s->tmp1, &s->flag);
+                break;
+            }
+            case FIN_BI_OMEGA: {  // NV = 4: <t, s>, <t, t>
+                s->tmp1[0] = acc[0];
+                s->tmp1[1] = acc[NV > 1 ? 1 : 0];
+                s->tmp2[0] = acc[NV > 2 ? 2 : 0];
+                s->tmp2[1] = acc[NV > 3 ? 3 : 0];
+                cx_div(s->omega, s->tmp1, s->tmp2, &s->flag);
+                break;
+            }
+            case FIN_BI_RESID: {
+                s->resid = acc[0];
+                if (ra.fin_arg) s->halt |= bicg_test(s, HALT_NAN, HALT_CONV);
+                break;
+            }
+            case FIN_BI_BETA: {
+                s->rho_next[0] = acc[0];
+                s->rho_next[1] = acc[NV > 1 ? 1 : 0];
+                if (bicg_stuck(s->rho_next)) {
+                    s->halt |= HALT_STUCK;
+                    break;
+                }
+                bicg_beta(s);
+                if (ra.fin_arg) s->halt_next |= bicg_test(s, HALT_NAN_NEXT, HALT_CONV_NEXT);
+                break;
+            }
+            case FIN_BIS_INIT: {
+                s->alpha[0] = s->omega[0] = s->rho[0] = 1.0;
+                s->alpha[1] = s->omega[1] = s->rho[1] = 0.0;
+                break;
+            }
+            case FIN_BIS_RHO: {
+                s->rho_next[0] = acc[0];
+                s->rho_next[1] = acc[NV > 1 ? 1 : 0];
+                if (bicg_stuck(s->rho_next)) {
+                    s->halt |= HALT_STUCK;
+                    break;
+                }
+                bicg_beta(s);
                 break;
             }
         }

@@ -1079,11 +1079,274 @@ int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_p
     return status;
 }
 
+// ----------------------------------------------- BiCGStab, device-driven
+// The eo BiCGStab above (fast and save variants; the same operations in the
+// same order, the same stopping and stuck tests, the same returned iterate)
+// with every scalar kept on the device.  The last block of each reduction
+// computes alpha, omega, beta, rho and applies the tests (FIN_BI_* in
+// reduce.cuh, rounded as the host's complex arithmetic); the BLAS read their
+// coefficients from device memory; a one-thread kernel at the end of each
+// iteration copies |r|^2 and the halt bits into a pinned ring slot, which the
+// host reads one iteration behind the queue.  When a test fires it sets
+// SolverScalars::halt, and every later BLAS / dslash launch of the solve finds
+// it set and leaves at once (RedArgs::halt), so the iteration already queued
+// behind the stopping one changes nothing: the solve stops on exactly the
+// iterate the reference's loop returns.  A stop that needs the host (the
+// true-residual confirmation of the save variant and of rel_tol) clears the
+// halt and re-queues the iteration that was skipped.
+__global__ void bicg_end_kernel(SolverScalars* s, double* slot)
+{
+    if (threadIdx.x != 0) return;
+    const int h  = s->halt | s->halt_next;  // the next iteration's opening test takes effect
+    s->halt      = h;
+    s->halt_next = 0;
+    slot[0]      = s->resid;
+    int* w       = reinterpret_cast<int*>(slot + 1);
+    w[0]         = h;
+    w[1]         = s->flag;
+    __threadfence_system();
+}
+
+struct HaltScope {  // the context's launch predicate for the duration of a solve
+    c2q_ctx* ctx;
+    HaltScope(c2q_ctx* c, const int* h) : ctx(c) { ctx->halt_dev = h; }
+    ~HaltScope() { ctx->halt_dev = nullptr; }
+};
+
+int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solver_params* P,
+                 c2q_solve_report* rep, bool report_true_residual = true)
+{
+    c2q_ctx* ctx = sp.ctx;
+    std::vector<c2q_spinor_eo*> w;
+    int rc = sp.alloc(7, w);
+    if (rc) return rc;
+    c2q_spinor_eo *const p = w[0], *const rn = w[1], *const rhat = w[2], *const s = w[3], *const t = w[4],
+                         *const v = w[5], *const aux = w[6];
+    const bool save = P->solver == C2Q_SOLVER_BICGSTAB_SAVE;
+    SolveClock clock(ctx);
+    Cx bb{0, 0};
+    rc = sp.dot(b, b, &bb);
+    if (rc) return rc;
+    const double b2  = bb.re;
+    const double thr = stop_threshold(P, b2);
+    SolverScalars* sc = ctx->scalars;
+    SolverScalars init{};
+    init.thr = thr;
+    rc       = write_sc(ctx, init);
+    if (rc) return rc;
+
+    auto blas = [&](int op, c2q_spinor_eo* out, Coef a, const c2q_spinor_eo* X, Coef bc, const c2q_spinor_eo* Y,
+                    const c2q_spinor_eo* Z, int dot = 0, int fin = FIN_STORE_RESULT, int fin_arg = 0) {
+        BlasSpec q;
+        q.op      = op;
+        q.out     = out;
+        q.a       = a;
+        q.x       = X;
+        q.b       = bc;
+        q.y       = Y;
+        q.z       = Z;
+        q.dot     = dot;
+        q.fin     = fin;
+        q.fin_arg = fin_arg;
+        return launch_blas(ctx, q);
+    };
+    const Coef one = coef_host(1.0, 0.0), none = coef_host(0.0, 0.0);
+    // (x, y) reductions into a finisher: dot 1 = <x,y>, dot 3 = <x,y> and <x,x>
+    auto dot = [&](const c2q_spinor_eo* X, const c2q_spinor_eo* Y, int kind, int fin, int fin_arg = 0) {
+        return blas(B_SAXPY, nullptr, none, X, none, Y, nullptr, kind, fin, fin_arg);
+    };
+    // sweeps of one operator application (Aee-type 2, QplusQminus_eo 4)
+    const int A = sp.op == C2Q_OP_QPLUSQMINUS_EO ? 4 : 2;
+    const int R = P->iter_refresh;
+
+    // bicgstab.cpp:612-723
+    auto fast_iter = [&](int it, bool refresh) -> int {
+        int e = 0;
+        if (refresh) {
+            e = sp.apply(rn, x);
+            if (!e) e = blas(B_SAXPY, p, one, rn, none, b, nullptr);  // p = b - rn
+            if (!e) e = copy_field(ctx, rhat, p);
+            if (!e) e = copy_field(ctx, rn, p);
+            if (!e) e = dot(rhat, rn, 3, FIN_BI_REFRESH);  // rho = (rhat, rn); resid = (rn, rn); the test
+        }
+        if (!e) e = sp.apply(v, p);
+        if (!e) e = dot(rhat, v, 1, FIN_BI_ALPHA);
+        if (!e) e = blas(B_SAXPY, s, coef_dev(sc->alpha), v, none, rn, nullptr);  // s = rn - alpha v
+        if (!e) e = sp.apply(t, s);
+        if (!e) e = dot(t, s, 3, FIN_BI_OMEGA);
+        if (!e) e = blas(B_SAXSBYPZ, x, coef_dev(sc->alpha), p, coef_dev(sc->omega), s, x);
+        if (!e)  // rn = s - omega t with resid = |rn|^2 for the next iteration's test
+            e = blas(B_SAXPY, rn, coef_dev(sc->omega), t, none, s, nullptr, 2, FIN_BI_RESID, 0);
+        if (!e) e = dot(rhat, rn, 1, FIN_BI_BETA, (it + 1) % R != 0);
+        if (!e) e = blas(B_SAXSBYPZ, p, coef_dev(sc->beta), p, coef_dev(sc->tmp2), v, rn);
+        return e;
+    };
+    // bicgstab.cpp:445-505 (x is updated before rn here: the two updates are independent)
+    auto save_iter = [&](int it, bool refresh) -> int {
+        (void)it;
+        int e = 0;
+        if (refresh) {
+            e = sp.zero(v);
+            if (!e) e = sp.zero(p);
+            if (!e) e = sp.apply(rn, x);
+            if (!e) e = blas(B_SAXPY, rn, one, rn, none, b, nullptr, 2, FIN_BIS_INIT);  // rn = b - rn; 1, 1, 1
+            if (!e) e = copy_field(ctx, rhat, rn);
+        }
+        if (!e) e = dot(rhat, rn, 1, FIN_BIS_RHO);
+        if (!e) e = blas(B_SAXSBYPZ, p, coef_dev(sc->beta), p, coef_dev(sc->tmp2), v, rn);
+        if (!e) e = sp.apply(v, p);
+        if (!e) e = dot(rhat, v, 1, FIN_BI_ALPHA);
+        if (!e) e = blas(B_SAXPY, s, coef_dev(sc->alpha), v, none, rn, nullptr);
+        if (!e) e = sp.apply(t, s);
+        if (!e) e = dot(t, s, 3, FIN_BI_OMEGA);
+        if (!e) e = blas(B_SAXSBYPZ, x, coef_dev(sc->alpha), p, coef_dev(sc->omega), s, x);
+        if (!e) e = blas(B_SAXPY, rn, coef_dev(sc->omega), t, none, s, nullptr, 2, FIN_BI_RESID, 1);
+        return e;
+    };
+    double* const ring_h = ctx->host_pinned + 32;
+    double* const ring_d = ctx->host_pinned_dev + 32;
+    auto push = [&](int k) -> int {
+        bicg_end_kernel<<<1, 32, 0, ctx->stream>>>(sc, ring_d + 2 * (k % 4));
+        ctx->launches++;
+        C2Q_CUDA(ctx, cudaGetLastError());
+        C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[k % 4], ctx->stream));
+        return C2Q_OK;
+    };
+    auto pop = [&](int k, double* r, int* h) -> int {
+        C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[k % 4]));
+        *r = ring_h[2 * (k % 4)];
+        memcpy(h, ring_h + 2 * (k % 4) + 1, sizeof(int));
+        return C2Q_OK;
+    };
+    // the true-residual confirmation (save variant, rel_tol); unpredicated
+    auto confirmed = [&](bool* ok) -> int {
+        ctx->halt_dev = nullptr;
+        int e         = sp.apply(aux, x);
+        if (!e) e = blas(B_SAXPY, aux, one, aux, none, b, nullptr, 2, FIN_STORE_RESULT);
+        double tr[2] = {0, 0};
+        if (!e) e = read_scalars(ctx, ctx->red_result, 2, tr);
+        ctx->halt_dev = &sc->halt;
+        const double lim = P->rel_tol > 0 ? std::max(P->rel_tol * P->rel_tol * b2, P->prec > 0 ? P->prec : 0.0)
+                                          : P->prec;
+        *ok = tr[0] < lim;
+        return e;
+    };
+
+    HaltScope scope(ctx, &sc->halt);
+    int status = C2Q_DID_NOT_SOLVE, iters = P->cgmax, executed = 0, resume = -1;
+    bool skip_refresh = false;
+    bool refreshed[4] = {};
+    double resid      = std::numeric_limits<double>::quiet_NaN();
+    // What a halted slot q means (bits h): 1 stop, 2 resume at `resume`.
+    auto settle = [&](int q, int h) -> int {
+        const int sweeps_q = (refreshed[q % 4] ? A : 0) + 2 * A;  // all of iteration q
+        if (h & HALT_STUCK) {  // fast: after the x update; save: at the top
+            executed += save ? (refreshed[q % 4] ? A : 0) : sweeps_q;
+            status = C2Q_SOLVER_STUCK;
+            iters  = q;
+            return 1;
+        }
+        if (h & HALT_NAN) {  // fast: the refresh's test; save: the end of q
+            executed += save ? sweeps_q : A;
+            status = C2Q_SOLVER_STUCK;
+            iters  = q;
+            return 1;
+        }
+        int j;
+        if (save) {
+            executed += sweeps_q;
+            j = q;
+        } else if (h & HALT_CONV) {  // the test of refresh iteration q
+            executed += A;
+            j = q;
+        } else {  // NAN_NEXT / CONV_NEXT: the test at the top of q + 1
+            executed += sweeps_q;
+            j = q + 1;
+            if (j >= P->cgmax) return 1;  // the reference leaves its loop first
+            if (h & HALT_NAN_NEXT) {
+                status = C2Q_SOLVER_STUCK;
+                iters  = j;
+                return 1;
+            }
+        }
+        bool ok = true;
+        if (save || P->rel_tol > 0) {
+            const int s0 = sp.sweeps;
+            rc           = confirmed(&ok);
+            executed += sp.sweeps - s0;
+            if (rc) return -1;
+        }
+        if (ok) {
+            status = j;
+            iters  = j;
+            return 1;
+        }
+        // the iterated residual drifted: clear the halt and carry on where the reference does
+        SolverScalars hs;
+        rc = read_sc(ctx, &hs);
+        if (rc) return -1;
+        hs.halt = hs.halt_next = 0;
+        rc                     = write_sc(ctx, hs);
+        if (rc) return -1;
+        if (save) {
+            resume = q + 1;
+        } else {
+            resume       = j;
+            skip_refresh = (h & HALT_CONV) != 0;  // its refresh ran; the rest of it did not
+        }
+        return 2;
+    };
+    int k = 0, first = 0;
+    for (;;) {
+        const bool more = k < P->cgmax;
+        if (more) {
+            const bool refresh = k % R == 0 && !skip_refresh;
+            skip_refresh       = false;
+            refreshed[k % 4]   = refresh;
+            rc                 = save ? save_iter(k, refresh) : fast_iter(k, refresh);
+            if (!rc) rc = push(k);
+            if (rc) return rc;
+        }
+        if (k > first) {  // slot k - 1: read one iteration behind the queue
+            int h = 0;
+            rc    = pop(k - 1, &resid, &h);
+            if (rc) return rc;
+            if (h) {
+                const int r = settle(k - 1, h);
+                if (r < 0) return rc;
+                if (r == 1) break;
+                k = first = resume;
+                continue;
+            }
+            executed += (refreshed[(k - 1) % 4] ? A : 0) + 2 * A;
+        }
+        if (!more) break;
+        ++k;
+    }
+    C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->halt_dev = nullptr;
+    double r2t    = 0;  // the defect correction skips this: it forms the FP64 true residual itself
+    if (report_true_residual) {
+        rc = sp.apply(aux, x);
+        if (!rc) rc = blas(B_SAXPY, aux, one, aux, none, b, nullptr, 2, FIN_STORE_RESULT);
+        double tr[2] = {0, 0};
+        if (!rc) rc = read_scalars(ctx, ctx->red_result, 2, tr);
+        if (rc) return rc;
+        r2t = tr[0];
+        executed += A;
+    }
+    sp.sweeps = executed;
+    finish_report(rep, status, iters, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), executed);
+    if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
+    if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "BiCGStab stuck (NaN residual or vanishing rho)");
+    return status;
+}
+
 int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b,
                   double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
 {
     EoSpace sp{ctx, &x->lat, op, g, gk64_for(g, P->use_rec12), kappa, mubar, action};
-    return bicgstab_generic(sp, x, const_cast<c2q_spinor_eo*>(b), P, rep);
+    return bicgstab_dev(sp, x, const_cast<c2q_spinor_eo*>(b), P, rep);
 }
 
 // Mixed-precision BiCGStab (no counterpart in the reference, whose solvers run
@@ -1150,7 +1413,7 @@ int bicgstab_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, c
         EoSpace sp{ctx, &x->lat, op, g, gk, kappa, mubar, action};
         sp.prec = PB;
         c2q_solve_report ir{};
-        const int st = bicgstab_generic(sp, ein, rin, &in, &ir, false);
+        const int st = bicgstab_dev(sp, ein, rin, &in, &ir, false);
         if (st < 0 && st != C2Q_SOLVER_STUCK && st != C2Q_DID_NOT_SOLVE) return st;
         sweeps += sp.sweeps;
         iters += ir.iterations;
