@@ -39,17 +39,21 @@ enum BlasOp : int {
     B_COPY,             // out = x
     B_GAMMA5,           // out = g5 x
     B_DIAG,             // out = diag(f1, f2) x   (a = f1, b = f2)
+    B_BICG_XR,          // BiCGStab: out = a x + b y + out, out2 = y - b z, with |out2|^2 and
+                        // <w, out2> (dot 4)
 };
 
 // Field arguments of one BLAS launch; any may be unused.
 template <int P>
 struct BlasArgs {
     SpinorPtr<P> out, x, y, z;
+    SpinorPtr<P> w, out2;  // B_BICG_XR only
     Coef a, b;
     int n, stride;
     int op;
     int dot;          // 0 none, 1 <x,y> (conj(x) y, no output write), 2 |out|^2,
-                      // 3 <x,y> and <x,x> in one pass (no output write)
+                      // 3 <x,y> and <x,x> in one pass (no output write),
+                      // 4 (B_BICG_XR) |out2|^2 and <w, out2>
     RedArgs red;
 };
 
@@ -60,7 +64,33 @@ __global__ void __launch_bounds__(BLAS_THREADS) blas_kernel(const BlasArgs<P> A)
     using R      = typename Prec<P>::R;
     const int i  = blockIdx.x * blockDim.x + threadIdx.x;
     double dv[4] = {0.0, 0.0, 0.0, 0.0};
-    if (i < A.n) {
+    if (i < A.n && A.op == B_BICG_XR) {
+        // bicgstab.cpp:694-702: x = alpha p + omega s + x; rn = s - omega t;
+        // then |rn|^2 and (rhat, rn)
+        const Cplx<double> a = coef_value(A.a), b = coef_value(A.b);
+        const Cplx<R> ar = cmk<R>((R)a.re, (R)a.im), br = cmk<R>((R)b.re, (R)b.im);
+        Cplx<R> xv[12], yv[12], r[12];
+        SpinorIO<P>::load(A.x, A.stride, i, xv);
+        SpinorIO<P>::load(A.y, A.stride, i, yv);
+        SpinorIO<P>::load(A.out, A.stride, i, r);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) r[k] = (cmul(yv[k], br) + cmul(xv[k], ar)) + r[k];
+        SpinorIO<P>::store(A.out, A.stride, i, r);
+        SpinorIO<P>::load(A.z, A.stride, i, xv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) r[k] = yv[k] - cmul(xv[k], br);
+        SpinorIO<P>::store(A.out2, A.stride, i, r);
+        // (the reductions use the values computed here: a load of what this kernel
+        // just stored could come through the non-coherent read-only path stale)
+        SpinorIO<P>::load(A.w, A.stride, i, yv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            dv[0] += (double)r[k].re * r[k].re + (double)r[k].im * r[k].im;
+            const Cplx<R> p = cmulc(yv[k], r[k]);
+            dv[2] += (double)p.re;
+            dv[3] += (double)p.im;
+        }
+    } else if (i < A.n) {
         Cplx<R> xv[12], r[12];
         if (A.dot == 1 || A.dot == 3) {
             Cplx<R> yv[12];
@@ -124,7 +154,7 @@ __global__ void __launch_bounds__(BLAS_THREADS) blas_kernel(const BlasArgs<P> A)
                 for (int k = 0; k < 12; ++k) dv[0] += (double)r[k].re * r[k].re + (double)r[k].im * r[k].im;
         }
     }
-    if (A.dot == 3) {
+    if (A.dot == 3 || A.dot == 4) {
         __shared__ double smem4[128];
         block_sum<4>(dv, smem4);
         finish_reduction<4>(dv, A.red, smem4);

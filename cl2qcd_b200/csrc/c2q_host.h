@@ -204,6 +204,8 @@ struct BlasSpec {
     Coef a{0, 0, nullptr, 1}, b{0, 0, nullptr, 1};
     c2q_spinor_eo* out = nullptr;
     const c2q_spinor_eo *x = nullptr, *y = nullptr, *z = nullptr;
+    const c2q_spinor_eo* w = nullptr;  // B_BICG_XR
+    c2q_spinor_eo* out2    = nullptr;  // B_BICG_XR
     int dot = 0;
     int fin = FIN_STORE_RESULT;
     int fin_arg = 0;

@@ -536,6 +536,8 @@ static int blas_typed(c2q_ctx* ctx, const BlasSpec& s, const c2q_spinor_eo* ref)
     A.x      = sptr<P>(s.x);
     A.y      = sptr<P>(s.y);
     A.z      = sptr<P>(s.z);
+    A.w      = sptr<P>(s.w);
+    A.out2   = sptr<P>(s.out2);
     A.a      = s.a;
     A.b      = s.b;
     A.n      = ref->geom.seo;
@@ -543,8 +545,8 @@ static int blas_typed(c2q_ctx* ctx, const BlasSpec& s, const c2q_spinor_eo* ref)
     A.op     = s.op;
     A.dot    = s.dot;
     const int blocks = (A.n + BLAS_THREADS - 1) / BLAS_THREADS;
-    if (s.dot) {  // dot 3 reduces four doubles per block
-        int rc = ensure_partials(ctx, s.dot == 3 ? 2 * (size_t)blocks : (size_t)blocks);
+    if (s.dot) {  // dot 3 and 4 reduce four doubles per block
+        int rc = ensure_partials(ctx, s.dot >= 3 ? 2 * (size_t)blocks : (size_t)blocks);
         if (rc) return rc;
     }
     A.red         = red_args(ctx, s.fin);
@@ -559,7 +561,9 @@ int launch_blas(c2q_ctx* ctx, const BlasSpec& s)
 {
     const c2q_spinor_eo* ref = s.out ? s.out : s.x;
     if (!ref || !s.x) return fail(ctx, C2Q_BAD_ARG, "null field");
-    for (const c2q_spinor_eo* f : {(const c2q_spinor_eo*)s.out, s.x, s.y, s.z})
+    if (s.op == B_BICG_XR && (!s.out || !s.y || !s.z || !s.w || !s.out2 || s.dot != 4))
+        return fail(ctx, C2Q_BAD_ARG, "B_BICG_XR needs out, x, y, z, w, out2 and dot 4");
+    for (const c2q_spinor_eo* f : {(const c2q_spinor_eo*)s.out, s.x, s.y, s.z, s.w, (const c2q_spinor_eo*)s.out2})
         if (f && (f->prec != ref->prec || !same_lattice(f->lat, ref->lat)))
             return fail(ctx, C2Q_BAD_ARG, "fields differ in precision or lattice");
     switch (ref->prec) {

@@ -84,6 +84,7 @@ enum Finisher : int {
                          // fin_arg: the next iteration's opening test (it is no refresh)
     FIN_BIS_INIT   = 9,  // save refresh: alpha = omega = rho = 1
     FIN_BIS_RHO    = 10, // save: rho_next = (rhat, rn), stuck test, beta, tmp2 = -beta omega, rho
+    FIN_BI_XR      = 11, // fast, NV = 4 (|rn|^2, 0, (rhat, rn)): FIN_BI_RESID then FIN_BI_BETA
 };
 
 struct RedArgs {
@@ -263,6 +264,18 @@ __device__ __forceinline__ void finish_group(const RedArgs& ra, double* smem, in
             case FIN_BI_BETA: {
                 s->rho_next[0] = acc[0];
                 s->rho_next[1] = acc[NV > 1 ? 1 : 0];
+                if (bicg_stuck(s->rho_next)) {
+                    s->halt |= HALT_STUCK;
+                    break;
+                }
+                bicg_beta(s);
+                if (ra.fin_arg) s->halt_next |= bicg_test(s, HALT_NAN_NEXT, HALT_CONV_NEXT);
+                break;
+            }
+            case FIN_BI_XR: {
+                s->resid       = acc[0];
+                s->rho_next[0] = acc[NV > 2 ? 2 : 0];
+                s->rho_next[1] = acc[NV > 3 ? 3 : 0];
                 if (bicg_stuck(s->rho_next)) {
                     s->halt |= HALT_STUCK;
                     break;

@@ -823,6 +823,11 @@ struct EoSpace {
     {
         return apply_operator(ctx, op, out, g, gk, in, kappa, mubar, action, t1, t2, DotSpec{}, &sweeps);
     }
+    // the same with a reduction fused into the last sweep
+    int apply_dot(V out, V in, const DotSpec& d)
+    {
+        return apply_operator(ctx, op, out, g, gk, in, kappa, mubar, action, t1, t2, d, &sweeps);
+    }
     int saxpy(V out, Cx a, V x, V y)
     {
         BlasSpec sp;
@@ -1158,8 +1163,13 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
     // sweeps of one operator application (Aee-type 2, QplusQminus_eo 4)
     const int A = sp.op == C2Q_OP_QPLUSQMINUS_EO ? 4 : 2;
     const int R = P->iter_refresh;
+    DotSpec alpha_dot;  // (rhat, A p) reduced in the operator's last sweep
+    alpha_dot.mode = DOT_Y;
+    alpha_dot.y    = rhat;
+    alpha_dot.fin  = FIN_BI_ALPHA;
 
-    // bicgstab.cpp:612-723
+    // bicgstab.cpp:612-723 (the x update, the rn update and the two
+    // reductions that follow them run as one pass, B_BICG_XR)
     auto fast_iter = [&](int it, bool refresh) -> int {
         int e = 0;
         if (refresh) {
@@ -1169,15 +1179,26 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
             if (!e) e = copy_field(ctx, rn, p);
             if (!e) e = dot(rhat, rn, 3, FIN_BI_REFRESH);  // rho = (rhat, rn); resid = (rn, rn); the test
         }
-        if (!e) e = sp.apply(v, p);
-        if (!e) e = dot(rhat, v, 1, FIN_BI_ALPHA);
+        if (!e) e = sp.apply_dot(v, p, alpha_dot);  // v = A p; tmp1 = (rhat, v); alpha
         if (!e) e = blas(B_SAXPY, s, coef_dev(sc->alpha), v, none, rn, nullptr);  // s = rn - alpha v
         if (!e) e = sp.apply(t, s);
         if (!e) e = dot(t, s, 3, FIN_BI_OMEGA);
-        if (!e) e = blas(B_SAXSBYPZ, x, coef_dev(sc->alpha), p, coef_dev(sc->omega), s, x);
-        if (!e)  // rn = s - omega t with resid = |rn|^2 for the next iteration's test
-            e = blas(B_SAXPY, rn, coef_dev(sc->omega), t, none, s, nullptr, 2, FIN_BI_RESID, 0);
-        if (!e) e = dot(rhat, rn, 1, FIN_BI_BETA, (it + 1) % R != 0);
+        if (!e) {  // x += alpha p + omega s; rn = s - omega t; |rn|^2, (rhat, rn): beta and the tests
+            BlasSpec q;
+            q.op      = B_BICG_XR;
+            q.out     = x;
+            q.a       = coef_dev(sc->alpha);
+            q.x       = p;
+            q.b       = coef_dev(sc->omega);
+            q.y       = s;
+            q.z       = t;
+            q.w       = rhat;
+            q.out2    = rn;
+            q.dot     = 4;
+            q.fin     = FIN_BI_XR;
+            q.fin_arg = (it + 1) % R != 0;
+            e         = launch_blas(ctx, q);
+        }
         if (!e) e = blas(B_SAXSBYPZ, p, coef_dev(sc->beta), p, coef_dev(sc->tmp2), v, rn);
         return e;
     };
@@ -1194,8 +1215,7 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
         }
         if (!e) e = dot(rhat, rn, 1, FIN_BIS_RHO);
         if (!e) e = blas(B_SAXSBYPZ, p, coef_dev(sc->beta), p, coef_dev(sc->tmp2), v, rn);
-        if (!e) e = sp.apply(v, p);
-        if (!e) e = dot(rhat, v, 1, FIN_BI_ALPHA);
+        if (!e) e = sp.apply_dot(v, p, alpha_dot);
         if (!e) e = blas(B_SAXPY, s, coef_dev(sc->alpha), v, none, rn, nullptr);
         if (!e) e = sp.apply(t, s);
         if (!e) e = dot(t, s, 3, FIN_BI_OMEGA);

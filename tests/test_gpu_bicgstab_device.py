@@ -85,3 +85,32 @@ def test_dslash_applications_counted_once(port, system):
     L, g, gf, b = _prob(port, c2q, system)
     j, _, rep = _solve(c2q, system, L, gf, b, "bicgstab", 1000)
     assert rep["dslash_applications"] == 2 * (1 + 2 * j + 1), (j, rep)
+
+
+@pytest.mark.parametrize("variant", ["bicgstab", "bicgstab_save"])
+@pytest.mark.parametrize("precision", [32, 16])
+@pytest.mark.parametrize("shape", [(8, 4), (4, 8)])
+def test_mixed_iterations_track_fp64(port, system, variant, precision, shape):
+    """The inner BiCGStab on FP32 / FP16 fields (fused x / rn update with its two
+    reductions, (rhat, v) reduced in the operator's last sweep) needs about the
+    iterations of the FP64 solve in total over its defect corrections, from a zero
+    and from a cold start: an inner iteration that reduced stale or wrong values
+    would still end in a converged outer solve, but only after many more."""
+    import cl2qcd_b200 as c2q
+    ns, nt = shape
+    L, g, gf, b = _prob(port, c2q, system, ns, nt)
+    add = c2q.AdditionalParameters(0.14, 2 * 0.14 * 0.05)
+    its = {}
+    for prec in (64, precision):
+        for cold in (False, True):
+            X, B = c2q.Spinorfield_eo(system, L), c2q.Spinorfield_eo(system, L, b)
+            if cold:
+                system.lib.c2q_spinor_eo_cold(X.h)
+            rep = {}
+            c2q.host.bicgstab(X, c2q.host.Aee(), gf, B,
+                              c2q.SolverParameters(solver=variant, prec=0.0, rel_tol=1e-11, cgmax=2000,
+                                                   precision=prec), add, rep)
+            assert rep["true_resid_rel"] <= 1e-11, rep
+            its[prec, cold] = rep["iterations"]
+    for cold in (False, True):
+        assert its[precision, cold] <= 1.3 * its[64, cold] + 5, its
