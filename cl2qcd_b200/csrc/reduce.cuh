@@ -161,6 +161,104 @@ __device__ __forceinline__ void store_partial(const double v[NV], const RedArgs&
         for (int k = 0; k < NV; ++k) ra.partials[index * NV + k] = v[k];
 }
 
+// What the last block's thread 0 does with the group's sum (RedArgs::fin).
+template <int NV>
+__device__ __forceinline__ void finish_apply(const RedArgs& ra, const double acc[NV])
+{
+    SolverScalars* s = ra.sc;
+    switch (ra.fin) {
+        case FIN_STORE_RESULT:
+#pragma unroll
+            for (int k = 0; k < NV; ++k) ra.result[k] = acc[k];
+            break;
+        case FIN_CG_ALPHA: {
+            s->rho[0] = acc[0];
+            s->rho[1] = NV > 1 ? acc[NV > 1 ? 1 : 0] : 0.0;
+            cdiv_store(s->alpha, s->omega, s->rho, &s->flag);
+            break;
+        }
+        case FIN_CG_BETA: {
+            s->rho_next[0] = acc[0];
+            s->rho_next[1] = 0.0;
+            s->resid       = acc[0];
+            cdiv_store(s->beta, s->rho_next, s->omega, &s->flag);
+            s->omega[0] = s->rho_next[0];
+            s->omega[1] = s->rho_next[1];
+            break;
+        }
+        case FIN_CG_OMEGA: {
+            s->omega[0] = acc[0];
+            s->omega[1] = 0.0;
+            s->resid    = acc[0];
+            break;
+        }
+        case FIN_BI_REFRESH: {  // NV = 4: <rhat, rn>, <rhat, rhat> with rhat = rn
+            s->rho[0] = acc[0];
+            s->rho[1] = acc[NV > 1 ? 1 : 0];
+            s->resid  = acc[NV > 2 ? 2 : 0];
+            s->halt |= bicg_test(s, HALT_NAN, HALT_CONV);
+            break;
+        }
+        case FIN_BI_ALPHA: {
+            s->tmp1[0] = acc[0];
+            s->tmp1[1] = acc[NV > 1 ? 1 : 0];
+            cx_div(s->alpha, s->rho, s->tmp1, &s->flag);
+            break;
+        }
+        case FIN_BI_OMEGA: {  // NV = 4: <t, s>, <t, t>
+            s->tmp1[0] = acc[0];
+            s->tmp1[1] = acc[NV > 1 ? 1 : 0];
+            s->tmp2[0] = acc[NV > 2 ? 2 : 0];
+            s->tmp2[1] = acc[NV > 3 ? 3 : 0];
+            cx_div(s->omega, s->tmp1, s->tmp2, &s->flag);
+            break;
+        }
+        case FIN_BI_RESID: {
+            s->resid = acc[0];
+            if (ra.fin_arg) s->halt |= bicg_test(s, HALT_NAN, HALT_CONV);
+            break;
+        }
+        case FIN_BI_BETA: {
+            s->rho_next[0] = acc[0];
+            s->rho_next[1] = acc[NV > 1 ? 1 : 0];
+            if (bicg_stuck(s->rho_next)) {
+                s->halt |= HALT_STUCK;
+                break;
+            }
+            bicg_beta(s);
+            if (ra.fin_arg) s->halt_next |= bicg_test(s, HALT_NAN_NEXT, HALT_CONV_NEXT);
+            break;
+        }
+        case FIN_BI_XR: {
+            s->resid       = acc[0];
+            s->rho_next[0] = acc[NV > 2 ? 2 : 0];
+            s->rho_next[1] = acc[NV > 3 ? 3 : 0];
+            if (bicg_stuck(s->rho_next)) {
+                s->halt |= HALT_STUCK;
+                break;
+            }
+            bicg_beta(s);
+            if (ra.fin_arg) s->halt_next |= bicg_test(s, HALT_NAN_NEXT, HALT_CONV_NEXT);
+            break;
+        }
+        case FIN_BIS_INIT: {
+            s->alpha[0] = s->omega[0] = s->rho[0] = 1.0;
+            s->alpha[1] = s->omega[1] = s->rho[1] = 0.0;
+            break;
+        }
+        case FIN_BIS_RHO: {
+            s->rho_next[0] = acc[0];
+            s->rho_next[1] = acc[NV > 1 ? 1 : 0];
+            if (bicg_stuck(s->rho_next)) {
+                s->halt |= HALT_STUCK;
+                break;
+            }
+            bicg_beta(s);
+            break;
+        }
+    }
+}
+
 // Called by every thread of every block after block_sum (value in thread 0).
 // Batched launches reduce per group: block b belongs to group b % G (one
 // group per right-hand side), each group has its own ticket ra.ticket[grp]
@@ -208,98 +306,7 @@ __device__ __forceinline__ void finish_group(const RedArgs& ra, double* smem, in
     block_sum<NV>(acc, smem);
     if (threadIdx.x == 0) {
         ra.ticket[grp] = 0u;
-        SolverScalars* s = ra.sc;
-        switch (ra.fin) {
-            case FIN_STORE_RESULT:
-#pragma unroll
-                for (int k = 0; k < NV; ++k) ra.result[k] = acc[k];
-                break;
-            case FIN_CG_ALPHA: {
-                s->rho[0] = acc[0];
-                s->rho[1] = NV > 1 ? acc[NV > 1 ? 1 : 0] : 0.0;
-                cdiv_store(s->alpha, s->omega, s->rho, &s->flag);
-                break;
-            }
-            case FIN_CG_BETA: {
-                s->rho_next[0] = acc[0];
-                s->rho_next[1] = 0.0;
-                s->resid       = acc[0];
-                cdiv_store(s->beta, s->rho_next, s->omega, &s->flag);
-                s->omega[0] = s->rho_next[0];
-                s->omega[1] = s->rho_next[1];
-                break;
-            }
-            case FIN_CG_OMEGA: {
-                s->omega[0] = acc[0];
-                s->omega[1] = 0.0;
-                s->resid    = acc[0];
-                break;
-            }
-            case FIN_BI_REFRESH: {  // NV = 4: <rhat, rn>, <rhat, rhat> with rhat = rn
-                s->rho[0] = acc[0];
-                s->rho[1] = acc[NV > 1 ? 1 : 0];
-                s->resid  = acc[NV > 2 ? 2 : 0];
-                s->halt |= bicg_test(s, HALT_NAN, HALT_CONV);
-                break;
-            }
-            case FIN_BI_ALPHA: {
-                s->tmp1[0] = acc[0];
-                s->tmp1[1] = acc[NV > 1 ? 1 : 0];
-                cx_div(s->alpha, s->rho, s->tmp1, &s->flag);
-                break;
-            }
-            case FIN_BI_OMEGA: {  // NV = 4: <t, s>, <t, t>
-                s->tmp1[0] = acc[0];
-                s->tmp1[1] = acc[NV > 1 ? 1 : 0];
-                s->tmp2[0] = acc[NV > 2 ? 2 : 0];
-                s->tmp2[1] = acc[NV > 3 ? 3 : 0];
-                cx_div(s->omega, s->tmp1, s->tmp2, &s->flag);
-                break;
-            }
-            case FIN_BI_RESID: {
-                s->resid = acc[0];
-                if (ra.fin_arg) s->halt |= bicg_test(s, HALT_NAN, HALT_CONV);
-                break;
-            }
-            case FIN_BI_BETA: {
-                s->rho_next[0] = acc[0];
-                s->rho_next[1] = acc[NV > 1 ? 1 : 0];
-                if (bicg_stuck(s->rho_next)) {
-                    s->halt |= HALT_STUCK;
-                    break;
-                }
-                bicg_beta(s);
-                if (ra.fin_arg) s->halt_next |= bicg_test(s, HALT_NAN_NEXT, HALT_CONV_NEXT);
-                break;
-            }
-            case FIN_BI_XR: {
-                s->resid       = acc[0];
-                s->rho_next[0] = acc[NV > 2 ? 2 : 0];
-                s->rho_next[1] = acc[NV > 3 ? 3 : 0];
-                if (bicg_stuck(s->rho_next)) {
-                    s->halt |= HALT_STUCK;
-                    break;
-                }
-                bicg_beta(s);
-                if (ra.fin_arg) s->halt_next |= bicg_test(s, HALT_NAN_NEXT, HALT_CONV_NEXT);
-                break;
-            }
-            case FIN_BIS_INIT: {
-                s->alpha[0] = s->omega[0] = s->rho[0] = 1.0;
-                s->alpha[1] = s->omega[1] = s->rho[1] = 0.0;
-                break;
-            }
-            case FIN_BIS_RHO: {
-                s->rho_next[0] = acc[0];
-                s->rho_next[1] = acc[NV > 1 ? 1 : 0];
-                if (bicg_stuck(s->rho_next)) {
-                    s->halt |= HALT_STUCK;
-                    break;
-                }
-                bicg_beta(s);
-                break;
-            }
-        }
+        finish_apply<NV>(ra, acc);
         __threadfence();
     }
 }

@@ -182,6 +182,36 @@ def test_two_sources_per_thread_is_bitwise_the_same(port, system, O, nsrc, rec12
         assert np.linalg.norm(r - srcs[k]) / np.linalg.norm(srcs[k]) <= 1.5e-10
 
 
+@pytest.mark.parametrize("shape", [(8, 8), (6, 8), (4, 12)])
+def test_every_sweep_choice_is_bitwise_the_same(port, system, O, shape):
+    """The FP16 mixed-precision CG (temporal gauge, 12-real links, fused x / r
+    updates) gives bitwise the same solution and iterations with every launch
+    choice (both configurations, one block per tile or grid-stride).  6^3x8 and
+    4^3x12 end in a ragged last tile."""
+    import cl2qcd_b200 as c2q
+    ns, nt = shape
+    L, g, gf = _problem(port, c2q, system, ns, nt, 0.3, 5)
+    add = c2q.AdditionalParameters(0.15, 2 * 0.15 * 0.01)
+    src = c2q.host.generate_source(L.seo, "gaussian", 77)
+    B = c2q.Spinorfield_eo(system, L, src)
+    P = c2q.SolverParameters(solver="cg", prec=0.0, rel_tol=1e-10, cgmax=5000, precision=16, use_rec12=True)
+    out = {}
+    try:
+        for choice in (0, 1, 2, 3):
+            system.set_sweep_choice(choice)
+            X = c2q.Spinorfield_eo(system, L)
+            rep = {}
+            c2q.host.cg(X, c2q.host.QplusQminus_eo(), gf, B, P, add, rep)
+            out[choice] = (X.dump(), rep["iterations"])
+    finally:
+        system.set_sweep_choice(-1)
+    for choice in (1, 2, 3):
+        assert out[choice][1] == out[0][1], (choice, out[choice][1], out[0][1])
+        assert np.array_equal(out[choice][0], out[0][0]), choice
+    r = port.apply(O.OP_QPQM_EO, out[0][0], g, 0.15, 2 * 0.15 * 0.01)
+    assert np.linalg.norm(r - src) / np.linalg.norm(src) <= 1.5e-10
+
+
 def test_sweep_choice_falls_back_where_it_does_not_apply(port, system, O):
     """Choice 4 on an FP32 batch (no two-per-thread kernel) runs choice 0."""
     import cl2qcd_b200 as c2q
