@@ -65,6 +65,9 @@ struct c2q_ctx {
     std::map<std::vector<int>, TuneEntry> tune;
     c2q::SolverScalars* tune_scratch = nullptr;  // reductions of tuning launches land here
     bool autotune = true;
+    // dependent launches of the solver-loop kernels (launch_dep); environment
+    // C2Q_DEPENDENT_LAUNCH=0 turns them off for new contexts
+    bool pdl = true;
     int force_choice = -1;  // >= 0: every paired-site sweep uses this choice where it applies
     // launch predicate of a device-driven solve (SolverScalars::halt): while set,
     // every reducing BLAS and dslash launch skips its work once *halt_dev != 0

@@ -24,7 +24,45 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 namespace c2q {
+
+// ---------------------------------------------------- dependent launches
+// The kernels of the solver loops are launched with programmatic stream
+// serialization: the next kernel on the stream may be scheduled while this one
+// drains (its last wave, the last block's reduction finisher), and it waits on
+// the device, at entry, until this one has completed and its writes are
+// visible.  pdl_enter() is that wait (a no-op for an ordinary launch) followed
+// by the signal that lets the next kernel be scheduled once every block of
+// this one is running.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+// Launch `kern` (whose blocks begin with pdl_enter) on stream s, as a
+// dependent launch when pdl is set.
+template <typename... K, typename... A>
+inline cudaError_t launch_dep(bool pdl, void (*kern)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              A&&... args)
+{
+    if (!pdl) {
+        kern<<<grid, block, smem, s>>>(std::forward<A>(args)...);
+        return cudaGetLastError();
+    }
+    cudaLaunchAttribute at[1];
+    at[0].id                                         = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg                           = {};
+    cfg.gridDim                                      = grid;
+    cfg.blockDim                                     = block;
+    cfg.dynamicSmemBytes                             = smem;
+    cfg.stream                                       = s;
+    cfg.attrs                                        = at;
+    cfg.numAttrs                                     = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
 
 // ------------------------------------------------------------------------
 // complex helpers (compute type R = double or float)

@@ -194,6 +194,7 @@ int ensure_partials(c2q_ctx* ctx, size_t blocks)
 __global__ void pinned_copy_kernel(const unsigned* __restrict__ src, size_t spitch, unsigned* __restrict__ dst,
                                    size_t dpitch, int width, int height)
 {
+    pdl_enter();
     for (int r = blockIdx.x; r < height; r += gridDim.x)
         for (int c = threadIdx.x; c < width; c += blockDim.x) dst[(size_t)r * dpitch + c] = src[(size_t)r * spitch + c];
 }
@@ -202,11 +203,10 @@ int pinned_copy(c2q_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t 
 {
     if (width % 4 || dpitch % 4 || spitch % 4 || height < 1) return fail(ctx, C2Q_BAD_ARG, "pinned_copy: word sizes");
     const int blocks = height < 16 ? height : 16;
-    pinned_copy_kernel<<<blocks, 32, 0, ctx->stream>>>(static_cast<const unsigned*>(src), spitch / 4,
-                                                       static_cast<unsigned*>(dst), dpitch / 4, (int)(width / 4),
-                                                       height);
+    C2Q_CUDA(ctx, launch_dep(ctx->pdl, pinned_copy_kernel, dim3(blocks), dim3(32), 0, ctx->stream,
+                             static_cast<const unsigned*>(src), (size_t)(spitch / 4), static_cast<unsigned*>(dst),
+                             (size_t)(dpitch / 4), (int)(width / 4), height));
     ctx->launches++;
-    C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
 }
 
@@ -728,6 +728,7 @@ C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream)
     c2q_ctx* ctx = new c2q_ctx();
     ctx->device  = device;
     if (const char* at = getenv("C2Q_AUTOTUNE")) ctx->autotune = at[0] != '0';
+    if (const char* pd = getenv("C2Q_DEPENDENT_LAUNCH")) ctx->pdl = pd[0] != '0';
     int rc       = C2Q_OK;
     auto chk     = [&](cudaError_t e, const char* w) {
         if (e != cudaSuccess && rc == C2Q_OK) rc = cuda_fail(ctx, e, w);

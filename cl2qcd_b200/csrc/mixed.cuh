@@ -63,6 +63,7 @@ __device__ __forceinline__ C2 caxpy2(C2 a, float2 cre, float2 cim, float2 ncim, 
 template <int PB>
 __global__ void __launch_bounds__(MIX_THREADS) mix_update_kernel(const MixArgs A)
 {
+    pdl_enter();
     const int nrhs     = A.nrhs;
     const int rhs      = nrhs == 1 ? 0 : (int)(blockIdx.x % (unsigned)nrhs);
     const int blk      = nrhs == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nrhs);
@@ -96,6 +97,7 @@ __global__ void __launch_bounds__(MIX_THREADS) mix_update_kernel(const MixArgs A
 template <int PB>
 __global__ void __launch_bounds__(MIX_THREADS) mix_p_kernel(const MixArgs A)
 {
+    pdl_enter();
     const int nrhs     = A.nrhs;
     const int rhs      = nrhs == 1 ? 0 : (int)(blockIdx.x % (unsigned)nrhs);
     const int blk      = nrhs == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)nrhs);

@@ -218,6 +218,7 @@ static int pk_launch(c2q_ctx* ctx, const c2q_gauge* g, int gkind, const PkBatch&
         R.result = nullptr;
     }
     prm.nrhs       = B.n;
+    prm.pdl        = ctx->pdl;
     prm.gauge      = g->store[gkind].data;
     prm.g          = pk_geom(ref->geom);
     prm.c          = hop_coef(ref->lat, B.kappa);

@@ -65,6 +65,7 @@ struct PkParams {
     int tg;                 // the gauge field is in the temporal gauge (PH_TG)
     double lam_re, lam_im;  // PH_TG: weight of the T hop leaving the last time slice
     RedArgs red;
+    int pdl;                // launched as a dependent launch (launch_dep)
 };
 
 // hop weight k (pairs) and its negations
@@ -501,6 +502,7 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
     static_assert(S::STAGES == 2 || S::STAGES == 3, "the prologue below issues one or two stages");
     static_assert(DOT != DOT_XUPD || EPI != EPI_AXPY, "the solution update shares the EPI_AXPY operand slot");
     constexpr bool RED = DOT != DOT_NONE && DOT != DOT_XUPD;  // a reduction is fused
+    pdl_enter();
     if (halted(prm.red)) return;  // a stopped device-driven solve: every block leaves
     extern __shared__ uint4 ring[];
     uint4* mine     = ring + threadIdx.x;

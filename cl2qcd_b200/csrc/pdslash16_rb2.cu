@@ -15,7 +15,7 @@ static void pk2_go(const PkParams<16>& prm, int blocks, cudaStream_t s)
         cudaFuncSetAttribute(pdslash2_kernel<NL, EPI, DOT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr_set[dev] = true;
     }
-    pdslash2_kernel<NL, EPI, DOT><<<blocks, PK_THREADS, smem, s>>>(prm);
+    launch_dep(prm.pdl != 0, pdslash2_kernel<NL, EPI, DOT>, dim3(blocks), dim3(PK_THREADS), smem, s, prm);
 }
 
 template <int NL>

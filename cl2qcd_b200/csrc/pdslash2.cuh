@@ -130,6 +130,7 @@ __global__ void __launch_bounds__(PK_THREADS, Pk2Stage<NL>::MINB) pdslash2_kerne
     static_assert(DOT != DOT_XUPD || EPI != EPI_AXPY, "the solution update shares the EPI_AXPY operand slot");
     constexpr bool RED = DOT != DOT_NONE && DOT != DOT_XUPD;
     constexpr int T    = PK_THREADS;
+    pdl_enter();
     if (halted(prm.red)) return;  // a stopped device-driven solve: every block leaves
     extern __shared__ uint4 ring[];
     uint4* mine     = ring + threadIdx.x;

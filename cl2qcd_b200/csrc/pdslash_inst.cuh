@@ -21,7 +21,7 @@ static void pk_go(const PkParams<P>& prm, int blocks, cudaStream_t s)
                              (int)smem);
         attr_set[dev] = true;
     }
-    pdslash_kernel<P, NL, EPI, DOT, PH, CFG><<<blocks, PK_THREADS, smem, s>>>(prm);
+    launch_dep(prm.pdl != 0, pdslash_kernel<P, NL, EPI, DOT, PH, CFG>, dim3(blocks), dim3(PK_THREADS), smem, s, prm);
 }
 
 template <int P, int NL, int PH, int CFG>

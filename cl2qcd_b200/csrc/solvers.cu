@@ -445,9 +445,8 @@ int mix_update_batch(c2q_ctx* ctx, const MixBatch& B)
     A.red.result   = ctx->red_result;
     A.red.sc       = ctx->scalars;
     A.red.fin      = FIN_CG_BETA;
-    mix_update_kernel<PB><<<blocks, MIX_THREADS, 0, ctx->stream>>>(A);
+    C2Q_CUDA(ctx, launch_dep(ctx->pdl, mix_update_kernel<PB>, dim3(blocks), dim3(MIX_THREADS), 0, ctx->stream, A));
     ctx->launches++;
-    C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
 }
 
@@ -456,9 +455,8 @@ int mix_p_batch(c2q_ctx* ctx, const MixBatch& B)
 {
     const MixArgs A  = mix_args(B);
     const int blocks = (A.H + MIX_THREADS - 1) / MIX_THREADS * B.n;
-    mix_p_kernel<PB><<<blocks, MIX_THREADS, 0, ctx->stream>>>(A);
+    C2Q_CUDA(ctx, launch_dep(ctx->pdl, mix_p_kernel<PB>, dim3(blocks), dim3(MIX_THREADS), 0, ctx->stream, A));
     ctx->launches++;
-    C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
 }
 
