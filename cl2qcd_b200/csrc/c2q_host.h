@@ -45,6 +45,14 @@ struct c2q_ctx {
     size_t staging_cap     = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t ring_ev[4] = {};  // residual ring of the pipelined solvers
+    // The pipelined solvers copy each iteration's residual into ring_dev on the
+    // context's stream (device memory only) and forward it to pinned host memory
+    // on `monitor`, so the solve never waits on a write across PCIe, which a large
+    // transfer of another stream can hold up; ring_ev[k] completes when slot k
+    // has reached the host, mon_ev[k] when it is in ring_dev.
+    cudaStream_t monitor   = nullptr;
+    cudaEvent_t mon_ev[4]  = {};
+    double* ring_dev       = nullptr;  // 4 slots x 16 right-hand sides x 4 doubles
     // optional per-launch dslash timing (c2q_ctx_profile)
     bool profiling = false;
     struct Timed {
@@ -182,7 +190,12 @@ int ensure_staging(c2q_ctx* ctx, size_t bytes);
 // of a pinned host buffer, by a one-block kernel on the context's stream:
 // `height` rows of `width` bytes, rows `dpitch` / `spitch` bytes apart.
 int pinned_copy(c2q_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
-                int height = 1);
+                int height = 1, cudaStream_t stream = nullptr);
+// Residual ring slot k (n rows of `width` bytes at src, row pitch spitch): into
+// ring_dev on the context's stream, then to the pinned host buffer dst_host_dev
+// (the device alias of a pinned slot) on the monitor stream; ring_ev[k % 4]
+// completes when the host can read it.
+int ring_push(c2q_ctx* ctx, int k, double* dst_host_dev, const void* src, size_t spitch, size_t width, int n);
 int ensure_partials(c2q_ctx* ctx, size_t blocks);
 
 template <int P>

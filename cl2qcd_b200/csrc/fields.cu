@@ -199,14 +199,29 @@ __global__ void pinned_copy_kernel(const unsigned* __restrict__ src, size_t spit
         for (int c = threadIdx.x; c < width; c += blockDim.x) dst[(size_t)r * dpitch + c] = src[(size_t)r * spitch + c];
 }
 
-int pinned_copy(c2q_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, int height)
+int pinned_copy(c2q_ctx* ctx, void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, int height,
+                cudaStream_t stream)
 {
     if (width % 4 || dpitch % 4 || spitch % 4 || height < 1) return fail(ctx, C2Q_BAD_ARG, "pinned_copy: word sizes");
     const int blocks = height < 16 ? height : 16;
-    C2Q_CUDA(ctx, launch_dep(ctx->pdl, pinned_copy_kernel, dim3(blocks), dim3(32), 0, ctx->stream,
+    C2Q_CUDA(ctx, launch_dep(ctx->pdl, pinned_copy_kernel, dim3(blocks), dim3(32), 0, stream ? stream : ctx->stream,
                              static_cast<const unsigned*>(src), (size_t)(spitch / 4), static_cast<unsigned*>(dst),
                              (size_t)(dpitch / 4), (int)(width / 4), height));
     ctx->launches++;
+    return C2Q_OK;
+}
+
+int ring_push(c2q_ctx* ctx, int k, double* dst_host_dev, const void* src, size_t spitch, size_t width, int n)
+{
+    if (width > 4 * sizeof(double) || n < 1 || n > 16) return fail(ctx, C2Q_BAD_ARG, "ring_push: slot size");
+    double* slot = ctx->ring_dev + (size_t)(k % 4) * 16 * 4;
+    int rc       = pinned_copy(ctx, slot, 4 * sizeof(double), src, spitch, width, n);
+    if (rc) return rc;
+    C2Q_CUDA(ctx, cudaEventRecord(ctx->mon_ev[k % 4], ctx->stream));
+    C2Q_CUDA(ctx, cudaStreamWaitEvent(ctx->monitor, ctx->mon_ev[k % 4], 0));
+    rc = pinned_copy(ctx, dst_host_dev, 4 * sizeof(double), slot, 4 * sizeof(double), width, n, ctx->monitor);
+    if (rc) return rc;
+    C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[k % 4], ctx->monitor));
     return C2Q_OK;
 }
 
@@ -749,6 +764,9 @@ C2Q_EXPORT int c2q_ctx_create(c2q_ctx** out, int device, void* cuda_stream)
     chk(cudaEventCreate(&ctx->ev0), "cudaEventCreate");
     chk(cudaEventCreate(&ctx->ev1), "cudaEventCreate");
     for (auto& e : ctx->ring_ev) chk(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    for (auto& e : ctx->mon_ev) chk(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    chk(cudaStreamCreateWithFlags(&ctx->monitor, cudaStreamNonBlocking), "cudaStreamCreate(monitor)");
+    chk(cudaMalloc(&ctx->ring_dev, 4 * 16 * 4 * sizeof(double)), "cudaMalloc(ring)");
     if (rc == C2Q_OK) {
         chk(cudaMemsetAsync(ctx->ticket, 0, 64 * sizeof(unsigned), ctx->stream), "memset");
         chk(cudaMemsetAsync(ctx->scalars, 0, sizeof(SolverScalars), ctx->stream), "memset");
@@ -774,7 +792,9 @@ C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx)
     if (!ctx) return C2Q_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->monitor) cudaStreamSynchronize(ctx->monitor);
     cudaFree(ctx->partials);
+    cudaFree(ctx->ring_dev);
     cudaFree(ctx->ticket);
     if (ctx->tune_scratch) cudaFree(ctx->tune_scratch);
     if (ctx->batch_ring) cudaFreeHost(ctx->batch_ring);
@@ -788,6 +808,9 @@ C2Q_EXPORT int c2q_ctx_destroy(c2q_ctx* ctx)
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     for (auto e : ctx->ring_ev)
         if (e) cudaEventDestroy(e);
+    for (auto e : ctx->mon_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->monitor) cudaStreamDestroy(ctx->monitor);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return C2Q_OK;

@@ -3,6 +3,7 @@
 // on top of the fused sweeps of fields.cu.
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <limits>
 #include <vector>
@@ -206,20 +207,19 @@ struct ResidRing {
     explicit ResidRing(c2q_ctx* c) : ctx(c) {}
     int push(int k)
     {
-        double* dslot = ctx->host_pinned_dev + 32 + 2 * (k % N);
-        int rc        = pinned_copy(ctx, dslot, 0, &ctx->scalars->resid, 0, sizeof(double));
-        if (!rc) rc = pinned_copy(ctx, dslot + 1, 0, &ctx->scalars->flag, 0, sizeof(int));
-        if (rc) return rc;
-        C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[k % N], ctx->stream));
-        return C2Q_OK;
+        // SolverScalars::resid, aux[2], flag: the first 28 bytes of the slot
+        static_assert(offsetof(SolverScalars, flag) == offsetof(SolverScalars, resid) + 3 * sizeof(double),
+                      "flag follows resid and aux[2]");
+        return ring_push(ctx, k, ctx->host_pinned_dev + 32 + 4 * (k % N), &ctx->scalars->resid, 0,
+                         4 * sizeof(double), 1);
     }
     int pop(int k, double* resid, int* flag)
     {
         C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[k % N]));
-        const double* slot = ctx->host_pinned + 32 + 2 * (k % N);
+        const double* slot = ctx->host_pinned + 32 + 4 * (k % N);
         *resid             = slot[0];
         int f;
-        memcpy(&f, slot + 1, sizeof(int));
+        memcpy(&f, slot + 3, sizeof(int));
         *flag = f;
         return C2Q_OK;
     }
@@ -695,10 +695,9 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
             if (rc) return rc;
         }
         for (int k : act) S[k].sweeps += per_apply;
-        rc = pinned_copy(ctx, ctx->batch_ring_dev + (size_t)(iter % 4) * PK_MAX_RHS * 4, 4 * sizeof(double),
-                         &dsc[0].resid, sizeof(SolverScalars), 4 * sizeof(double), n);
+        rc = ring_push(ctx, iter, ctx->batch_ring_dev + (size_t)(iter % 4) * PK_MAX_RHS * 4, &dsc[0].resid,
+                       sizeof(SolverScalars), 4 * sizeof(double), n);
         if (rc) return rc;
-        C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[iter % 4], ctx->stream));
         if (iter == 0) continue;
         C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[(iter - 1) % 4]));
         const double* prev = ctx->batch_ring + (size_t)((iter - 1) % 4) * PK_MAX_RHS * 4;
@@ -1088,26 +1087,20 @@ int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_p
 // with every scalar kept on the device.  The last block of each reduction
 // computes alpha, omega, beta, rho and applies the tests (FIN_BI_* in
 // reduce.cuh, rounded as the host's complex arithmetic); the BLAS read their
-// coefficients from device memory; a one-thread kernel at the end of each
-// iteration copies |r|^2 and the halt bits into a pinned ring slot, which the
-// host reads one iteration behind the queue.  When a test fires it sets
+// coefficients from device memory; at the end of each iteration |r|^2 and the
+// halt bits go to a ring slot (ring_push), which the host reads one iteration
+// behind the queue.  When a test fires it sets
 // SolverScalars::halt, and every later BLAS / dslash launch of the solve finds
 // it set and leaves at once (RedArgs::halt), so the iteration already queued
 // behind the stopping one changes nothing: the solve stops on exactly the
 // iterate the reference's loop returns.  A stop that needs the host (the
 // true-residual confirmation of the save variant and of rel_tol) clears the
 // halt and re-queues the iteration that was skipped.
-__global__ void bicg_end_kernel(SolverScalars* s, double* slot)
+__global__ void bicg_end_kernel(SolverScalars* s)
 {
     if (threadIdx.x != 0) return;
-    const int h  = s->halt | s->halt_next;  // the next iteration's opening test takes effect
-    s->halt      = h;
+    s->halt      = s->halt | s->halt_next;  // the next iteration's opening test takes effect
     s->halt_next = 0;
-    slot[0]      = s->resid;
-    int* w       = reinterpret_cast<int*>(slot + 1);
-    w[0]         = h;
-    w[1]         = s->flag;
-    __threadfence_system();
 }
 
 struct HaltScope {  // the context's launch predicate for the duration of a solve
@@ -1223,17 +1216,19 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
     };
     double* const ring_h = ctx->host_pinned + 32;
     double* const ring_d = ctx->host_pinned_dev + 32;
+    // slot: resid, aux[2], flag, halt -- the first 32 bytes from SolverScalars::resid
+    static_assert(offsetof(SolverScalars, halt) == offsetof(SolverScalars, resid) + 3 * sizeof(double) + sizeof(int),
+                  "halt follows resid, aux[2] and flag");
     auto push = [&](int k) -> int {
-        bicg_end_kernel<<<1, 32, 0, ctx->stream>>>(sc, ring_d + 2 * (k % 4));
+        bicg_end_kernel<<<1, 32, 0, ctx->stream>>>(sc);
         ctx->launches++;
         C2Q_CUDA(ctx, cudaGetLastError());
-        C2Q_CUDA(ctx, cudaEventRecord(ctx->ring_ev[k % 4], ctx->stream));
-        return C2Q_OK;
+        return ring_push(ctx, k, ring_d + 4 * (k % 4), &sc->resid, 0, 4 * sizeof(double), 1);
     };
     auto pop = [&](int k, double* r, int* h) -> int {
         C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[k % 4]));
-        *r = ring_h[2 * (k % 4)];
-        memcpy(h, ring_h + 2 * (k % 4) + 1, sizeof(int));
+        *r = ring_h[4 * (k % 4)];
+        memcpy(h, reinterpret_cast<const char*>(ring_h + 4 * (k % 4) + 3) + sizeof(int), sizeof(int));
         return C2Q_OK;
     };
     // the true-residual confirmation (save variant, rel_tol); unpredicated
