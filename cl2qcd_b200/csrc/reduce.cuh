@@ -85,6 +85,7 @@ enum Finisher : int {
     FIN_BIS_INIT   = 9,  // save refresh: alpha = omega = rho = 1
     FIN_BIS_RHO    = 10, // save: rho_next = (rhat, rn), stuck test, beta, tmp2 = -beta omega, rho
     FIN_BI_XR      = 11, // fast, NV = 4 (|rn|^2, 0, (rhat, rn)): FIN_BI_RESID then FIN_BI_BETA
+    FIN_BI_RHO     = 12, // rho = (rhat, rn) (rn replaced by a true residual)
 };
 
 struct RedArgs {
@@ -239,6 +240,11 @@ __device__ __forceinline__ void finish_apply(const RedArgs& ra, const double acc
             }
             bicg_beta(s);
             if (ra.fin_arg) s->halt_next |= bicg_test(s, HALT_NAN_NEXT, HALT_CONV_NEXT);
+            break;
+        }
+        case FIN_BI_RHO: {
+            s->rho[0] = acc[0];
+            s->rho[1] = acc[NV > 1 ? 1 : 0];
             break;
         }
         case FIN_BIS_INIT: {

@@ -847,10 +847,8 @@ struct EoSpace {
         sp.b   = coef_host(b.re, b.im);
         return launch_blas(ctx, sp);
     }
-    int copy(V to, V from) { return copy_field(ctx, to, from); }
     int zero(V f) { return c2q_spinor_eo_zero(f); }
     int dot(V x, V y, Cx* out) { return dot_read(ctx, x, y, out); }
-    int dot2(V x, V y, Cx* xy, Cx* xx) { return dot2_read(ctx, x, y, xy, xx); }
 };
 
 struct FullSpace {
@@ -1109,30 +1107,29 @@ struct HaltScope {  // the context's launch predicate for the duration of a solv
     ~HaltScope() { ctx->halt_dev = nullptr; }
 };
 
-int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solver_params* P,
-                 c2q_solve_report* rep, bool report_true_residual = true)
-{
-    c2q_ctx* ctx = sp.ctx;
-    std::vector<c2q_spinor_eo*> w;
-    int rc = sp.alloc(7, w);
-    if (rc) return rc;
-    c2q_spinor_eo *const p = w[0], *const rn = w[1], *const rhat = w[2], *const s = w[3], *const t = w[4],
-                         *const v = w[5], *const aux = w[6];
-    const bool save = P->solver == C2Q_SOLVER_BICGSTAB_SAVE;
-    SolveClock clock(ctx);
-    Cx bb{0, 0};
-    rc = sp.dot(b, b, &bb);
-    if (rc) return rc;
-    const double b2  = bb.re;
-    const double thr = stop_threshold(P, b2);
-    SolverScalars* sc = ctx->scalars;
-    SolverScalars init{};
-    init.thr = thr;
-    rc       = write_sc(ctx, init);
-    if (rc) return rc;
+// The device-driven iteration on an eo vector space: the field set, the
+// enqueueing of one fast or save iteration, and the residual ring.
+struct BicgLoop {
+    c2q_ctx* ctx;
+    EoSpace& sp;
+    SolverScalars* sc;
+    c2q_spinor_eo *p, *rn, *rhat, *s, *t, *v, *aux;
+    int A;  // sweeps of one operator application (Aee-type 2, QplusQminus_eo 4)
+    int R;  // refresh interval
+    DotSpec alpha_dot;
+    const Coef one = coef_host(1.0, 0.0), none = coef_host(0.0, 0.0);
 
-    auto blas = [&](int op, c2q_spinor_eo* out, Coef a, const c2q_spinor_eo* X, Coef bc, const c2q_spinor_eo* Y,
-                    const c2q_spinor_eo* Z, int dot = 0, int fin = FIN_STORE_RESULT, int fin_arg = 0) {
+    BicgLoop(EoSpace& space, const std::vector<c2q_spinor_eo*>& w, int refresh)
+        : ctx(space.ctx), sp(space), sc(space.ctx->scalars), p(w[0]), rn(w[1]), rhat(w[2]), s(w[3]), t(w[4]),
+          v(w[5]), aux(w[6]), A(space.op == C2Q_OP_QPLUSQMINUS_EO ? 4 : 2), R(refresh)
+    {
+        alpha_dot.mode = DOT_Y;  // (rhat, A p) reduced in the operator's last sweep
+        alpha_dot.y    = rhat;
+        alpha_dot.fin  = FIN_BI_ALPHA;
+    }
+    int blas(int op, c2q_spinor_eo* out, Coef a, const c2q_spinor_eo* X, Coef bc, const c2q_spinor_eo* Y,
+             const c2q_spinor_eo* Z, int dot = 0, int fin = FIN_STORE_RESULT, int fin_arg = 0)
+    {
         BlasSpec q;
         q.op      = op;
         q.out     = out;
@@ -1145,27 +1142,25 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
         q.fin     = fin;
         q.fin_arg = fin_arg;
         return launch_blas(ctx, q);
-    };
-    const Coef one = coef_host(1.0, 0.0), none = coef_host(0.0, 0.0);
+    }
     // (x, y) reductions into a finisher: dot 1 = <x,y>, dot 3 = <x,y> and <x,x>
-    auto dot = [&](const c2q_spinor_eo* X, const c2q_spinor_eo* Y, int kind, int fin, int fin_arg = 0) {
+    int dot(const c2q_spinor_eo* X, const c2q_spinor_eo* Y, int kind, int fin, int fin_arg = 0)
+    {
         return blas(B_SAXPY, nullptr, none, X, none, Y, nullptr, kind, fin, fin_arg);
-    };
-    // sweeps of one operator application (Aee-type 2, QplusQminus_eo 4)
-    const int A = sp.op == C2Q_OP_QPLUSQMINUS_EO ? 4 : 2;
-    const int R = P->iter_refresh;
-    DotSpec alpha_dot;  // (rhat, A p) reduced in the operator's last sweep
-    alpha_dot.mode = DOT_Y;
-    alpha_dot.y    = rhat;
-    alpha_dot.fin  = FIN_BI_ALPHA;
-
-    // bicgstab.cpp:612-723 (the x update, the rn update and the two
-    // reductions that follow them run as one pass, B_BICG_XR)
-    auto fast_iter = [&](int it, bool refresh) -> int {
+    }
+    // bicgstab.cpp:612-723 (the x update, the rn update and the two reductions
+    // that follow them run as one pass, B_BICG_XR).  refresh 2: x is zero, so
+    // rn = b without applying the operator.
+    int fast_iter(c2q_spinor_eo* x, const c2q_spinor_eo* b, int it, int refresh)
+    {
         int e = 0;
-        if (refresh) {
+        if (refresh == 2) {
+            e = copy_field(ctx, p, b);
+        } else if (refresh) {
             e = sp.apply(rn, x);
             if (!e) e = blas(B_SAXPY, p, one, rn, none, b, nullptr);  // p = b - rn
+        }
+        if (refresh) {
             if (!e) e = copy_field(ctx, rhat, p);
             if (!e) e = copy_field(ctx, rn, p);
             if (!e) e = dot(rhat, rn, 3, FIN_BI_REFRESH);  // rho = (rhat, rn); resid = (rn, rn); the test
@@ -1192,10 +1187,10 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
         }
         if (!e) e = blas(B_SAXSBYPZ, p, coef_dev(sc->beta), p, coef_dev(sc->tmp2), v, rn);
         return e;
-    };
+    }
     // bicgstab.cpp:445-505 (x is updated before rn here: the two updates are independent)
-    auto save_iter = [&](int it, bool refresh) -> int {
-        (void)it;
+    int save_iter(c2q_spinor_eo* x, const c2q_spinor_eo* b, bool refresh)
+    {
         int e = 0;
         if (refresh) {
             e = sp.zero(v);
@@ -1213,24 +1208,59 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
         if (!e) e = blas(B_SAXSBYPZ, x, coef_dev(sc->alpha), p, coef_dev(sc->omega), s, x);
         if (!e) e = blas(B_SAXPY, rn, coef_dev(sc->omega), t, none, s, nullptr, 2, FIN_BI_RESID, 1);
         return e;
-    };
-    double* const ring_h = ctx->host_pinned + 32;
-    double* const ring_d = ctx->host_pinned_dev + 32;
-    // slot: resid, aux[2], flag, halt -- the first 32 bytes from SolverScalars::resid
-    static_assert(offsetof(SolverScalars, halt) == offsetof(SolverScalars, resid) + 3 * sizeof(double) + sizeof(int),
-                  "halt follows resid, aux[2] and flag");
-    auto push = [&](int k) -> int {
+    }
+    // ring slot k: resid, aux[2], flag, halt -- the first 32 bytes from SolverScalars::resid
+    int push(int k)
+    {
+        static_assert(offsetof(SolverScalars, halt) ==
+                          offsetof(SolverScalars, resid) + 3 * sizeof(double) + sizeof(int),
+                      "halt follows resid, aux[2] and flag");
         bicg_end_kernel<<<1, 32, 0, ctx->stream>>>(sc);
         ctx->launches++;
         C2Q_CUDA(ctx, cudaGetLastError());
-        return ring_push(ctx, k, ring_d + 4 * (k % 4), &sc->resid, 0, 4 * sizeof(double), 1);
-    };
-    auto pop = [&](int k, double* r, int* h) -> int {
+        return ring_push(ctx, k, ctx->host_pinned_dev + 32 + 4 * (k % 4), &sc->resid, 0, 4 * sizeof(double), 1);
+    }
+    int pop(int k, double* r, int* h)
+    {
         C2Q_CUDA(ctx, cudaEventSynchronize(ctx->ring_ev[k % 4]));
-        *r = ring_h[4 * (k % 4)];
-        memcpy(h, reinterpret_cast<const char*>(ring_h + 4 * (k % 4) + 3) + sizeof(int), sizeof(int));
+        const double* slot = ctx->host_pinned + 32 + 4 * (k % 4);
+        *r                 = slot[0];
+        memcpy(h, reinterpret_cast<const char*>(slot + 3) + sizeof(int), sizeof(int));
         return C2Q_OK;
+    }
+};
+
+int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solver_params* P,
+                 c2q_solve_report* rep, bool report_true_residual = true)
+{
+    c2q_ctx* ctx = sp.ctx;
+    std::vector<c2q_spinor_eo*> w;
+    int rc = sp.alloc(7, w);
+    if (rc) return rc;
+    BicgLoop L(sp, w, P->iter_refresh);
+    c2q_spinor_eo* const aux = L.aux;
+    const bool save          = P->solver == C2Q_SOLVER_BICGSTAB_SAVE;
+    SolveClock clock(ctx);
+    Cx bb{0, 0};
+    rc = sp.dot(b, b, &bb);
+    if (rc) return rc;
+    const double b2  = bb.re;
+    const double thr = stop_threshold(P, b2);
+    SolverScalars* sc = ctx->scalars;
+    SolverScalars init{};
+    init.thr = thr;
+    rc       = write_sc(ctx, init);
+    if (rc) return rc;
+    const Coef one = L.one, none = L.none;
+    const int A    = L.A, R = L.R;
+    auto blas      = [&](int op, c2q_spinor_eo* out, Coef a, const c2q_spinor_eo* X, Coef bc,
+                    const c2q_spinor_eo* Y, const c2q_spinor_eo* Z, int dot = 0, int fin = FIN_STORE_RESULT) {
+        return L.blas(op, out, a, X, bc, Y, Z, dot, fin);
     };
+    auto fast_iter = [&](int it, bool refresh) { return L.fast_iter(x, b, it, refresh ? 1 : 0); };
+    auto save_iter = [&](int, bool refresh) { return L.save_iter(x, b, refresh); };
+    auto push      = [&](int k) { return L.push(k); };
+    auto pop       = [&](int k, double* r, int* h) { return L.pop(k, r, h); };
     // the true-residual confirmation (save variant, rel_tol); unpredicated
     auto confirmed = [&](bool* ok) -> int {
         ctx->halt_dev = nullptr;
@@ -1363,12 +1393,19 @@ int bicgstab_impl(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, co
 }
 
 // Mixed-precision BiCGStab (no counterpart in the reference, whose solvers run
-// in FP64): defect correction around the BiCGStab above.  Each outer step forms
-// the true residual r = b - A x in FP64, solves A e = r / |r| by BiCGStab on
-// FP32 or FP16 fields and links until that inner residual has dropped by
-// reliable_delta (or by what the stopping test still needs), and adds |r| e to x
-// in FP64.  The stopping test (prec / rel_tol) is applied to the FP64 true
-// residual; cgmax bounds the inner iterations of all steps together.
+// in FP64), with reliable updates: the device-driven BiCGStab iteration above
+// (fast variant) runs on FP32 or FP16 fields and links and accumulates its
+// solution increment xs there; whenever its iterated residual has dropped by
+// reliable_delta since the last update, or below the stopping threshold, x +=
+// xs in FP64 and the FP64 true residual r = b - A x replaces the iterated one
+// (with rho = (rhat, r)), and the iteration goes on with its search direction,
+// shadow residual and scalars kept -- the Krylov space survives the updates
+// (Sleijpen and van der Vorst's reliable updates for BiCGStab).  The stopping
+// test (prec / rel_tol) is applied to the FP64 true residual, confirmed on the
+// links as uploaded.  A vanishing rho restarts the iteration from the true
+// residual (twice in a row without progress: SolverStuck); cgmax bounds the
+// iterations.  The save variant's defining step, confirming convergence with
+// the true residual, is what every update does, so both settings run this.
 template <int PB>
 int bicgstab_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b,
                    double kappa, double mubar, int action, const c2q_solver_params* P, c2q_solve_report* rep)
@@ -1386,68 +1423,129 @@ int bicgstab_mixed(c2q_ctx* ctx, c2q_spinor_eo* x, int op, const c2q_gauge* g, c
     if (!rc) rc = make_fields(ctx, x->lat, PB, 2, FB, 0);
     if (rc) return rc;
     c2q_spinor_eo *r64 = &F64.f[0], *a64 = &F64.f[1], *b64 = &F64.f[2], *e64 = &F64.f[3];
-    c2q_spinor_eo *rin = &FB.f[0], *ein = &FB.f[1];
+    c2q_spinor_eo *rin = &FB.f[0], *xs = &FB.f[1];
+    EoSpace sp{ctx, &x->lat, op, g, gk, kappa, mubar, action};
+    sp.prec = PB;
+    std::vector<c2q_spinor_eo*> w;
+    rc = sp.alloc(7, w);
+    if (rc) return rc;
+    BicgLoop L(sp, w, 1 << 30);  // no periodic refresh: the reliable updates replace it
     double b2 = 0;
     rc        = norm2(ctx, b, &b2);
     if (rc) return rc;
     const double thr   = stop_threshold(P, b2);
     const double delta = P->reliable_delta > 0 && P->reliable_delta < 1 ? P->reliable_delta : 0.003;
-    c2q_solver_params in = *P;
-    in.rel_tol           = 0.0;
-    in.min_iter          = 0;
-    int iters = 0, steps = 0, sweeps = 0, status = C2Q_DID_NOT_SOLVE;
-    double r2 = 0;
-    for (;;) {
-        rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, gk64);
-        if (!rc && gk64 != G64 && r2 < thr)
-            rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, G64);
-        if (rc) return rc;
-        if (r2 != r2) {
-            status = C2Q_SOLVER_STUCK;
-            break;
-        }
-        if (r2 < thr || r2 == 0.0) {
-            status = iters;
-            break;
-        }
-        if (iters >= P->cgmax) break;
-        const double rn = std::sqrt(r2);
-        BlasSpec sc;  // a64 = r / |r|, then to the inner precision
-        sc.op  = B_SAX;
-        sc.out = a64;
-        sc.x   = r64;
-        sc.a   = coef_host(1.0 / rn, 0.0);
-        rc     = launch_blas(ctx, sc);
-        if (!rc) rc = launch_convert(ctx, rin, a64);
-        if (!rc) rc = c2q_spinor_eo_zero(ein);
-        if (rc) return rc;
-        in.cgmax = P->cgmax - iters;
-        in.prec  = std::max(delta * delta, 0.01 * thr / r2);
-        EoSpace sp{ctx, &x->lat, op, g, gk, kappa, mubar, action};
-        sp.prec = PB;
-        c2q_solve_report ir{};
-        const int st = bicgstab_dev(sp, ein, rin, &in, &ir, false);
-        if (st < 0 && st != C2Q_SOLVER_STUCK && st != C2Q_DID_NOT_SOLVE) return st;
-        sweeps += sp.sweeps;
-        iters += ir.iterations;
-        ++steps;
-        if (st == C2Q_SOLVER_STUCK && ir.iterations == 0) {
-            status = C2Q_SOLVER_STUCK;
-            break;
-        }
-        BlasSpec up;  // x += |r| e in FP64
+    int iters = 0, updates = 0, sweeps = 0, status = C2Q_DID_NOT_SOLVE, stuck_run = 0;
+    double r2 = 0, maxr = 0;
+
+    // x += xs in FP64, then r = b - A x; returns 1 when r meets the stopping test
+    auto reliable = [&](bool* conv) -> int {
+        *conv  = false;
+        int e  = launch_convert(ctx, e64, xs);
+        BlasSpec up;  // x = x - (-1) e
         up.op  = B_SAXPY;
         up.out = x;
         up.x   = e64;
         up.y   = x;
-        up.a   = coef_host(-rn, 0.0);
-        rc     = launch_convert(ctx, e64, ein);
-        if (!rc) rc = launch_blas(ctx, up);
+        up.a   = coef_host(-1.0, 0.0);
+        if (!e) e = launch_blas(ctx, up);
+        if (!e) e = c2q_spinor_eo_zero(xs);
+        if (!e) e = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, gk64);
+        if (!e && gk64 != G64 && r2 < thr)
+            e = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, G64);
+        if (e) return e;
+        *conv = r2 < thr || r2 == 0.0;
+        maxr  = std::sqrt(r2);
+        return C2Q_OK;
+    };
+    // a fresh start of the iteration from the FP64 residual: rin = r, xs = 0
+    SolverScalars init{};  // thr 0: the iteration never stops itself; the host tests the FP64 residual
+    auto restart = [&]() -> int {
+        int e = launch_convert(ctx, rin, r64);
+        if (!e) e = write_sc(ctx, init);
+        return e;
+    };
+
+    rc = c2q_spinor_eo_zero(xs);
+    if (!rc) rc = true_residual(ctx, op, g, x, b, kappa, mubar, action, r64, a64, b64, &r2, &sweeps, G64);
+    if (rc) return rc;
+    maxr = std::sqrt(r2);
+    if (r2 < thr || r2 == 0.0) {
+        status = 0;
+    } else if (r2 != r2) {
+        status = C2Q_SOLVER_STUCK;
+    } else {
+        rc = restart();
         if (rc) return rc;
+        HaltScope scope(ctx, &ctx->scalars->halt);
+        int refresh = 2, skip_upto = -1;
+        for (int k = 0;; ++k) {
+            const bool more = k < P->cgmax;
+            if (more) {
+                rc = L.fast_iter(xs, rin, k, refresh);
+                if (!rc) rc = L.push(k);
+                if (rc) return rc;
+                refresh = 0;
+            }
+            if (k == 0) continue;
+            double res = 0;
+            int h      = 0;
+            rc         = L.pop(k - 1, &res, &h);
+            if (rc) return rc;
+            if (k - 1 <= skip_upto) {  // queued before the last update, which took in what it did
+                if (!h) ++iters;        // (it ran, unless a halt stopped it)
+                if (!more) break;
+                continue;
+            }
+            ++iters;
+            const bool stuck = (h & HALT_STUCK) != 0;
+            if ((h & (HALT_NAN | HALT_NAN_NEXT)) || res != res) {
+                status = C2Q_SOLVER_STUCK;
+                break;
+            }
+            if (stuck || res < delta * delta * maxr * maxr || res < thr || !more) {
+                // an update after the iteration queued behind this one (or a
+                // restart where rho vanished); nothing is predicated meanwhile
+                ctx->halt_dev       = nullptr;
+                const double before = maxr;
+                bool conv           = false;
+                rc                  = reliable(&conv);
+                if (rc) return rc;
+                ++updates;
+                if (conv) {
+                    status = iters;
+                    break;
+                }
+                if (r2 != r2) {
+                    status = C2Q_SOLVER_STUCK;
+                    break;
+                }
+                if (!more) break;
+                if (stuck) {
+                    stuck_run = maxr < 0.5 * before ? 0 : stuck_run + 1;
+                    if (stuck_run >= 2) {
+                        status = C2Q_SOLVER_STUCK;
+                        break;
+                    }
+                    rc      = restart();
+                    refresh = 2;
+                } else {
+                    // the true residual replaces the iterated one: rn = r, rho = (rhat, rn)
+                    rc = launch_convert(ctx, L.rn, r64);
+                    if (!rc) rc = L.dot(L.rhat, L.rn, 1, FIN_BI_RHO);
+                }
+                if (rc) return rc;
+                ctx->halt_dev = &ctx->scalars->halt;
+                skip_upto     = k;
+            } else if (!more) {
+                break;
+            }
+        }
     }
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    sweeps += sp.sweeps;
     const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-    finish_report(rep, status, iters, steps, r2, b2 > 0 ? std::sqrt(r2 / b2) : 0.0, secs, sweeps);
+    finish_report(rep, status, iters, updates, r2, b2 > 0 ? std::sqrt(r2 / b2) : 0.0, secs, sweeps);
     if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
     if (status == C2Q_SOLVER_STUCK) fail(ctx, status, "mixed-precision BiCGStab stuck (NaN residual or vanishing rho)");
     return status;
