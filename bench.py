@@ -793,7 +793,7 @@ def main():
     # field and source at kappa 0.12 (below the free critical kappa 1/8: at kappa
     # 0.16 the non-Hermitian Aee of these near-unit links has eigenvalues around
     # the origin and BiCGStab does not converge): FP64
-    # against mixed precision (FP32 / FP16 inner, FP64 defect correction), each to
+    # against mixed precision (FP32 / FP16 inner, FP64 reliable updates), each to
     # the true residual 1e-10, timed over five solves after one untimed
     def bicgstab_section():
         kap = 0.12
@@ -820,7 +820,7 @@ def main():
                 continue
             sec = e0.elapsed_time(e1) / 1e3 / nrep_b
             out[key] = {"solves_per_s": 1.0 / sec, "iterations": rep["iterations"],
-                        "defect_corrections": rep["reliable_updates"], "true_resid_rel": rep["true_resid_rel"]}
+                        "reliable_updates": rep["reliable_updates"], "true_resid_rel": rep["true_resid_rel"]}
         if "solves_per_s" in out.get("mixed_fp16", {}) and "solves_per_s" in out.get("fp64", {}):
             out["speedup_mixed_fp16_vs_fp64"] = out["mixed_fp16"]["solves_per_s"] / out["fp64"]["solves_per_s"]
         return out

@@ -920,8 +920,7 @@ struct FullSpace {
 // physics/algorithms/solvers/bicgstab.cpp:566-733 (fast) and :401-564 (save);
 // scalars are read back every iteration as the reference does.
 template <class S>
-int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_params* P, c2q_solve_report* rep,
-                     bool report_true_residual = true)
+int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_params* P, c2q_solve_report* rep)
 {
     c2q_ctx* ctx = sp.ctx;
     std::vector<typename S::V> w;
@@ -1070,8 +1069,8 @@ int bicgstab_generic(S& sp, typename S::V x, typename S::V b, const c2q_solver_p
             }
         }
     }
-    double r2t = 0;  // the defect correction skips this: it forms the FP64 true residual itself
-    if (report_true_residual) rc = true_r2(&r2t);
+    double r2t = 0;
+    rc         = true_r2(&r2t);
     if (rc) return rc;
     finish_report(rep, status, iter, 0, resid, b2 > 0 ? std::sqrt(r2t / b2) : 0.0, clock.seconds(), sp.sweeps);
     if (status == C2Q_DID_NOT_SOLVE) fail(ctx, status, "Solver did not solve in solverMaxIterations iterations");
@@ -1231,7 +1230,7 @@ struct BicgLoop {
 };
 
 int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solver_params* P,
-                 c2q_solve_report* rep, bool report_true_residual = true)
+                 c2q_solve_report* rep)
 {
     c2q_ctx* ctx = sp.ctx;
     std::vector<c2q_spinor_eo*> w;
@@ -1368,8 +1367,8 @@ int bicgstab_dev(EoSpace& sp, c2q_spinor_eo* x, c2q_spinor_eo* b, const c2q_solv
     }
     C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     ctx->halt_dev = nullptr;
-    double r2t    = 0;  // the defect correction skips this: it forms the FP64 true residual itself
-    if (report_true_residual) {
+    double r2t    = 0;
+    {
         rc = sp.apply(aux, x);
         if (!rc) rc = blas(B_SAXPY, aux, one, aux, none, b, nullptr, 2, FIN_STORE_RESULT);
         double tr[2] = {0, 0};

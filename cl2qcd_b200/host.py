@@ -489,8 +489,8 @@ def point_source(n_sites: int, k: int) -> np.ndarray:
 
 def bicgstab(x, A, gf, b, params: SolverParameters, add: AdditionalParameters, report: dict | None = None) -> int:
     """solvers::bicgstab on eo fields (A an eo matrix) or on full fields (A a full-lattice matrix).
-    On eo fields, params.precision 32 or 16 runs it on FP32 / FP16 fields inside an FP64
-    defect correction (report["reliable_updates"] counts the corrections); full fields are FP64."""
+    On eo fields, params.precision 32 or 16 runs it on FP32 / FP16 fields with FP64 reliable
+    updates (report["reliable_updates"] counts them); full fields are FP64."""
     return _solve(x.system.lib.c2q_bicgstab, x, A, gf, b, params, add, report, x.system.lib.c2q_bicgstab_full)
 
 

@@ -382,11 +382,12 @@ C2Q_EXPORT int c2q_cg(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_sp
                       double mubar, int action, const c2q_solver_params* p, c2q_solve_report* report);
 /* solvers::bicgstab (physics/algorithms/solvers/bicgstab.hpp:42-57, bicgstab.cpp:384-733);
  * p->solver selects the fast (C2Q_SOLVER_BICGSTAB) or save (C2Q_SOLVER_BICGSTAB_SAVE) variant.
- * With p->precision 32 or 16 (no counterpart in the reference): that BiCGStab on
- * FP32 / FP16 fields and links inside an FP64 defect correction (each step solves
- * A e = r / |r| for the FP64 true residual r until the inner residual has dropped
- * by reliable_delta, then x += |r| e); the stopping test applies to the FP64 true
- * residual and report->reliable_updates counts the steps. */
+ * With p->precision 32 or 16 (no counterpart in the reference): the BiCGStab
+ * iteration on FP32 / FP16 fields and links with reliable updates (whenever its
+ * iterated residual has dropped by reliable_delta, x takes the accumulated
+ * increment in FP64 and the FP64 true residual replaces the iterated one; the
+ * search direction and shadow residual are kept); the stopping test applies to
+ * the FP64 true residual and report->reliable_updates counts the updates. */
 C2Q_EXPORT int c2q_bicgstab(c2q_spinor_eo* x, int op, const c2q_gauge* g, const c2q_spinor_eo* b, double kappa,
                             double mubar, int action, const c2q_solver_params* p, c2q_solve_report* report);
 /* Multi-right-hand-side CG on one operator: x[k], b[k] for k < nrhs (each

@@ -93,7 +93,7 @@ def test_dslash_applications_counted_once(port, system):
 def test_mixed_iterations_track_fp64(port, system, variant, precision, shape):
     """The inner BiCGStab on FP32 / FP16 fields (fused x / rn update with its two
     reductions, (rhat, v) reduced in the operator's last sweep) needs about the
-    iterations of the FP64 solve in total over its defect corrections, from a zero
+    iterations of the FP64 solve, over its reliable updates, from a zero
     and from a cold start: an inner iteration that reduced stale or wrong values
     would still end in a converged outer solve, but only after many more."""
     import cl2qcd_b200 as c2q

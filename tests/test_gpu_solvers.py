@@ -75,7 +75,7 @@ def test_bicgstab_matches_oracle(port, system, O, variant):
 @pytest.mark.parametrize("precision", [32, 16])
 @pytest.mark.parametrize("opname", ["Aee", "Qminus_eo"])
 def test_mixed_bicgstab_true_residual(port, system, O, variant, precision, opname):
-    """Mixed-precision BiCGStab (inner BiCGStab on FP32 / FP16 fields, FP64 defect correction)
+    """Mixed-precision BiCGStab (the iteration on FP32 / FP16 fields, FP64 reliable updates)
     reaches ||b - A x|| / ||b|| <= 1e-10, checked with the oracle operator, and agrees with the
     solution of the oracle's FP64 BiCGStab."""
     import cl2qcd_b200 as c2q
