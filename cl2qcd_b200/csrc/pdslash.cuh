@@ -29,6 +29,9 @@
 namespace c2q {
 
 constexpr int PK_THREADS = 128;
+// partials per thread and load round of the sweeps' reduction finisher (4096
+// tiles at 32^3x64: two rounds for the 128 threads of the last block)
+constexpr int PK_FINISH_ROUND = 16;
 
 // Fields of one right-hand side of a batch.
 struct PkRhs {
@@ -714,7 +717,7 @@ __global__ void __launch_bounds__(PK_THREADS, PkStage<P, NL, CFG>::MINB) pdslash
         RedArgs ra = prm.red;
         if (rr.sc) ra.sc = rr.sc;
         if (rr.result) ra.result = rr.result;
-        finish_group<2>(ra, smem, rhs, nrhs, prm.ntiles, G);
+        finish_group<2, PK_FINISH_ROUND>(ra, smem, rhs, nrhs, prm.ntiles, G);
     }
 }
 

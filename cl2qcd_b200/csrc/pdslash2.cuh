@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(PK_THREADS, Pk2Stage<NL>::MINB) pdslash2_kerne
             if (rr.sc) ra.sc = rr.sc;
             if (rr.result) ra.result = rr.result;
             if (r) __syncthreads();  // every thread has read the first group's flag before it is set again
-            finish_group<2>(ra, smem, 2 * pair + r, prm.nrhs, prm.ntiles, G);
+            finish_group<2, PK_FINISH_ROUND>(ra, smem, 2 * pair + r, prm.nrhs, prm.ntiles, G);
         }
     }
 }

@@ -276,7 +276,10 @@ __device__ __forceinline__ void finish_reduction(const double v[NV], const RedAr
 // The ticket and final sum of a group whose `nparts` partials sit at
 // partials[(m * G + grp) * NV], m < nparts, written by the `nblocks` blocks of
 // the group (grid-stride kernels write several partials per block).
-template <int NV>
+// ROUND: partials loaded per thread before they are added (the order of the
+// additions does not depend on it); wider rounds shorten this block's serial
+// tail, at ROUND * NV registers.
+template <int NV, int ROUND = 8>
 __device__ __forceinline__ void finish_group(const RedArgs& ra, double* smem, int grp, int G, int nparts, int nblocks)
 {
     __shared__ bool last;
@@ -290,22 +293,22 @@ __device__ __forceinline__ void finish_group(const RedArgs& ra, double* smem, in
     __threadfence();
     const int nb = nparts;
     // fixed-order sum of the group's partials: thread j takes partials
-    // j, j + blockDim.x, ... in rounds of 8 independent loads (this block runs
-    // alone at the end of the kernel, so its load latency is not hidden)
+    // j, j + blockDim.x, ... in rounds of ROUND independent loads (this block
+    // runs alone at the end of the kernel, so its load latency is not hidden)
     double acc[NV];
 #pragma unroll
     for (int k = 0; k < NV; ++k) acc[k] = 0.0;
     const int step = blockDim.x;
-    for (int m0 = threadIdx.x; m0 < nb; m0 += 8 * step) {
-        double t[8][NV];
+    for (int m0 = threadIdx.x; m0 < nb; m0 += ROUND * step) {
+        double t[ROUND][NV];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < ROUND; ++u) {
             const int m = m0 + u * step;
 #pragma unroll
             for (int k = 0; k < NV; ++k) t[u][k] = m < nb ? __ldcg(ra.partials + ((size_t)m * G + grp) * NV + k) : 0.0;
         }
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+        for (int u = 0; u < ROUND; ++u)
 #pragma unroll
             for (int k = 0; k < NV; ++k) acc[k] += t[u][k];
     }
