@@ -60,6 +60,7 @@ struct BlasArgs {
 template <int P>
 __global__ void __launch_bounds__(BLAS_THREADS) blas_kernel(const BlasArgs<P> A)
 {
+    pdl_enter();
     if (halted(A.red)) return;  // a stopped device-driven solve: every block leaves
     using R      = typename Prec<P>::R;
     const int i  = blockIdx.x * blockDim.x + threadIdx.x;
@@ -178,6 +179,7 @@ struct CgUpdateArgs {
 template <int P>
 __global__ void __launch_bounds__(BLAS_THREADS) cg_update_kernel(const CgUpdateArgs<P> A)
 {
+    pdl_enter();
     using R      = typename Prec<P>::R;
     const int i  = blockIdx.x * blockDim.x + threadIdx.x;
     double dv[2] = {0.0, 0.0};
@@ -214,6 +216,7 @@ struct CgPArgs {
 template <int P>
 __global__ void __launch_bounds__(BLAS_THREADS) cg_p_kernel(const CgPArgs<P> A)
 {
+    pdl_enter();
     using R     = typename Prec<P>::R;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.n) return;

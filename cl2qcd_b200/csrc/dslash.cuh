@@ -41,6 +41,7 @@ struct DslashParams {
     EpiArgs e;
     int out_parity;    // parity of the output sites: 0 = (x+y+z+t) even
     RedArgs red;
+    int pdl;           // launched as a dependent launch (launch_dep)
 };
 
 // multiply by c in {1, -1, i, -i}, encoded as K = 0, 1, 2, 3
@@ -182,6 +183,7 @@ __device__ __forceinline__ void do_direction(Cplx<typename Prec<P>::R> acc[12], 
 template <int P, int NL, int EPI, int DOT, int PH>
 __global__ void __launch_bounds__(128) dslash_kernel(const DslashParams<P> prm)
 {
+    pdl_enter();
     if (halted(prm.red)) return;  // a stopped device-driven solve: every block leaves
     using R       = typename Prec<P>::R;
     const Geom& g = prm.g;

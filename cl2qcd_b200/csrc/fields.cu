@@ -432,7 +432,7 @@ int gauge_drop_derived(c2q_gauge* g)
 template <int P, int NL, int EPI, int DOT, int PH>
 static void dslash_go(const DslashParams<P>& prm, int blocks, cudaStream_t s)
 {
-    dslash_kernel<P, NL, EPI, DOT, PH><<<blocks, 128, 0, s>>>(prm);
+    launch_dep(prm.pdl != 0, dslash_kernel<P, NL, EPI, DOT, PH>, dim3(blocks), dim3(128), 0, s, prm);
 }
 
 template <int P, int NL, int PH>
@@ -479,6 +479,7 @@ static int dslash_typed(c2q_ctx* ctx, const c2q_gauge* g, int gkind, c2q_spinor_
         if (rc) return rc;
     }
     prm.red = red_args(ctx, dot.fin);
+    prm.pdl = ctx->pdl;
     const bool r12 = gkind == G64R12 || gkind == G32R12 || gkind == G16R12;  // FP64 here
     c2q_ctx::Timed tm{};
     if (ctx->profiling) {
@@ -566,7 +567,7 @@ static int blas_typed(c2q_ctx* ctx, const BlasSpec& s, const c2q_spinor_eo* ref)
     }
     A.red         = red_args(ctx, s.fin);
     A.red.fin_arg = s.fin_arg;
-    blas_kernel<P><<<blocks, BLAS_THREADS, 0, ctx->stream>>>(A);
+    C2Q_CUDA(ctx, launch_dep(ctx->pdl, blas_kernel<P>, dim3(blocks), dim3(BLAS_THREADS), 0, ctx->stream, A));
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
@@ -604,7 +605,7 @@ static int cg_update_typed(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* r, con
     int rc = ensure_partials(ctx, blocks);
     if (rc) return rc;
     A.red = red_args(ctx, FIN_CG_BETA);
-    cg_update_kernel<P><<<blocks, BLAS_THREADS, 0, ctx->stream>>>(A);
+    C2Q_CUDA(ctx, launch_dep(ctx->pdl, cg_update_kernel<P>, dim3(blocks), dim3(BLAS_THREADS), 0, ctx->stream, A));
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
@@ -630,7 +631,7 @@ static int cg_p_typed(c2q_ctx* ctx, c2q_spinor_eo* p, const c2q_spinor_eo* r)
     A.n = p->geom.seo;
     A.stride = p->geom.stride;
     const int blocks = (A.n + BLAS_THREADS - 1) / BLAS_THREADS;
-    cg_p_kernel<P><<<blocks, BLAS_THREADS, 0, ctx->stream>>>(A);
+    C2Q_CUDA(ctx, launch_dep(ctx->pdl, cg_p_kernel<P>, dim3(blocks), dim3(BLAS_THREADS), 0, ctx->stream, A));
     ctx->launches++;
     C2Q_CUDA(ctx, cudaGetLastError());
     return C2Q_OK;
