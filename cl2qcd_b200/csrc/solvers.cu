@@ -472,6 +472,21 @@ int accumulate(c2q_ctx* ctx, c2q_spinor_eo* x, c2q_spinor_eo* xs, const c2q_spin
     return C2Q_OK;
 }
 
+// A reliable update's scalars: beta rescaled to the true residual r2 (the
+// search direction is kept), omega = resid = r2, alpha = 0 (the deferred x
+// update was accumulated).
+__global__ void mixed_rescale_kernel(SolverScalars* s, double r2)
+{
+    if (threadIdx.x != 0) return;
+    s->beta[0] *= r2 / s->resid;
+    s->beta[1] *= r2 / s->resid;
+    s->omega[0] = r2;
+    s->omega[1] = 0.0;
+    s->resid    = r2;
+    s->alpha[0] = 0.0;
+    s->alpha[1] = 0.0;
+}
+
 // Mixed-precision CG on a batch of right-hand sides that share the operator:
 // the right-hand sides iterate in lockstep (every sweep and vector update is
 // one launch over the active ones, so each link is read once per batch), each
@@ -553,13 +568,6 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
         const int rc1 = pinned_copy(ctx, dsc + k, 0, ctx->host_pinned_dev, 0, sizeof(SolverScalars));
         if (rc1) return rc1;
         C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        return C2Q_OK;
-    };
-    auto read_one = [&](int k, SolverScalars* h) -> int {
-        const int rc1 = pinned_copy(ctx, ctx->host_pinned_dev, 0, dsc + k, 0, sizeof(SolverScalars));
-        if (rc1) return rc1;
-        C2Q_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        memcpy(h, ctx->host_pinned, sizeof(SolverScalars));
         return C2Q_OK;
     };
 
@@ -722,9 +730,7 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 // reliable update in FP64 after iteration `iter`
                 // (an update expected to be the last one uses the uploaded links;
                 // one that converges unexpectedly on 12-real links is confirmed on them)
-                SolverScalars h;
-                rc = read_one(k, &h);
-                if (!rc) rc = take_out(k, fused ? nullptr : dsc + k);
+                rc = take_out(k, fused ? nullptr : dsc + k);
                 const int gk_upd = resid < s.thr ? G64 : gk64;
                 if (!rc)
                     rc = true_residual(ctx, op, g, x[k], b[k], kappa, mubar, action, r64, a64, b64, &s.r2, &s.sweeps,
@@ -745,16 +751,11 @@ int cg_mixed_batch(c2q_ctx* ctx, c2q_spinor_eo* const* x, int op, const c2q_gaug
                 rc = to_inner(rs[k], r64);
                 if (rc) return rc;
                 s.maxrr = std::sqrt(s.r2);
-                // keep the search direction; rescale beta to the true residual
-                h.beta[0] *= s.r2 / h.resid;
-                h.beta[1] *= s.r2 / h.resid;
-                h.omega[0] = s.r2;
-                h.omega[1] = 0.0;
-                h.resid    = s.r2;
-                h.alpha[0] = 0.0;  // the deferred x update was accumulated
-                h.alpha[1] = 0.0;
-                rc         = write_one(k, h);
-                if (rc) return rc;
+                // keep the search direction; rescale beta to the true residual (on
+                // the device: the scalars never cross to the host here)
+                mixed_rescale_kernel<<<1, 32, 0, ctx->stream>>>(dsc + k, s.r2);
+                ctx->launches++;
+                C2Q_CUDA(ctx, cudaGetLastError());
                 s.skip_upto = iter;
             }
         }
